@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""Benchmark of the CHR sampler on the genome-shaped workload.
+
+Workload (one "step" = one full sampling job): the seeded genome-shaped
+polytope n=2600 reactions, d=700, A=[T;-T] (m=5200), T 8% dense N(0,1),
+bounds log-uniform on [1,1000]; 16 chains x 12500 samples, thinning 116,
+pair-prob 0.3, start y=0, followed by the backmap V = T y + shift of all
+200,000 samples to n=2600.  Synthetic data stands in for a rounded
+genome-scale model (none ships with the reference).
+
+value  = chain-correct min-ESS / second of the timed job (ESS per dim summed
+         over de-interleaved chains, min over dims; seconds = sampling +
+         backmap with inputs resident in HBM), gated by split-R-hat and
+         bounds violations, which the line reports.
+e2e    = the same min-ESS over the job run from host buffers through the C
+         ABI: polytope upload, start points, sampling, backmap, and the
+         back-transformed samples copied to pinned host memory.
+roofline: the step kernel, algorithmic bytes per CHR step
+         4*m*(1+p_pair) + 4*d/thinning (one FP32 column of A per coordinate,
+         two per pair step, plus the amortised sample write) over its
+         CUDA-event duration, against MEASURED_PEAKS.json hbm_gbs.
+cpu_baseline: the CPU oracle (same algorithm, same tier, bit-identical
+         trajectory) on a bounded sample of the workload on the host cores;
+         its min-ESS/s is the GPU run's min-ESS per CHR step times the CPU's
+         CHR steps per second.
+
+`--impl reference` times the reference's own sampler (see _reference_arm).
+Multi-GPU (torchrun): each rank runs an independent replica with its own
+chain streams (weak scaling, no data-path collective); per-dim ESS sums are
+combined after timing.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "min-ESS/sec at split-R-hat<1.01, learned-rounded vs plain CHR, 1 B200"
+UNIT = "min-ESS/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+class Workload:
+    def __init__(self, a):
+        from naja_b200 import synth
+
+        self.n, self.d = a.n, a.d
+        g = synth.genome_shaped(n=a.n, d=a.d, density=0.08, seed_T=0, seed_u=1)
+        self.g = g
+        self.A, self.b, self.T, self.shift, self.start = g["A"], g["b"], g["T"], g["shift"], g["start"]
+        self.m = self.A.shape[0]
+        self.nchains, self.nspc, self.thin, self.pair = a.nchains, a.nspc, a.thinning, a.pair_prob
+        self.steps = self.nchains * self.nspc * self.thin
+        self.bytes_per_step = 4.0 * self.m * (1.0 + self.pair) + 4.0 * self.d / self.thin
+
+    def config(self, a):
+        return {"workload": f"genome-shaped polytope n={self.n} d={self.d} m={self.m}, {self.nchains} chains x "
+                            f"{self.nspc} samples, thinning {self.thin}, pair-prob {self.pair}, backmap to n={self.n}",
+                "n": self.n, "d": self.d, "m": self.m, "chains": self.nchains, "samples_per_chain": self.nspc,
+                "thinning": self.thin, "pair_prob": self.pair, "precision": a.precision,
+                "resync_interval": a.resync, "backmap": a.backmap_mode, "rng": "philox",
+                "l2": "256 MiB buffer written between timed steps"}
+
+
+def _gate(torch, W, samples_dev, ess, rhat, V_dev):
+    """split-R-hat and bounds checks on the fp32 output (outside the timed region)."""
+    A = torch.from_numpy(W.A).to(samples_dev.device)
+    b = torch.from_numpy(W.b).to(samples_dev.device)
+    tol = 1e-6 * torch.clamp(b.abs(), min=1.0)
+    viol = 0
+    worst = 0.0
+    for s0 in range(0, samples_dev.shape[0], 20000):
+        r = samples_dev[s0:s0 + 20000].double() @ A.T - b
+        viol += int((r > tol).sum())
+        worst = max(worst, float(r.max()))
+    # GEM bounds on <= 1000 back-transformed samples (bounds_check.cpp:8-39 rule, eps 1e-6)
+    step = max(1, V_dev.shape[0] // 1000)
+    v = V_dev[::step].double()
+    u = torch.from_numpy(W.g["u"]).to(v.device)
+    lo = torch.from_numpy(W.g["l"]).to(v.device)
+    gem = torch.maximum(lo - v - 1e-6, v - u - 1e-6)
+    return {"rhat_max": float(np.max(rhat)), "rhat_gate_1_01": bool(np.max(rhat) < 1.01),
+            "bounds_violations": viol, "bounds_worst": worst,
+            "gem_bounds_violations": int((gem > 0).sum()), "gem_bounds_checked": int(gem.numel())}
+
+
+def _cpu_baseline(W, a, min_ess_per_step):
+    import oracle.oracle as O
+
+    cores = min(os.cpu_count() or 1, W.nchains)
+    nspc = 2
+    t0 = time.perf_counter()
+    O.chr_run(W.A, W.b, W.start, nspc, W.thin, W.nchains, seed=a.seed, pair_prob=W.pair, resync_interval=a.resync,
+              precision=a.precision, threads=cores)
+    dt = time.perf_counter() - t0
+    nspc = max(2, min(W.nspc, int(nspc * a.cpu_seconds / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    O.chr_run(W.A, W.b, W.start, nspc, W.thin, W.nchains, seed=a.seed, pair_prob=W.pair, resync_interval=a.resync,
+              precision=a.precision, threads=cores)
+    dt = time.perf_counter() - t0
+    steps_s = W.nchains * nspc * W.thin / dt
+    return {"value": min_ess_per_step * steps_s, "unit": UNIT, "cores": cores, "kind": "port",
+            "steps_per_s": steps_s,
+            "sample": f"{W.nchains} chains x {nspc} samples (thinning {W.thin}) of the same workload, CPU oracle "
+                      f"{a.precision} tier, {cores} threads, {dt:.1f} s; min-ESS/s = GPU min-ESS per CHR step x "
+                      f"CPU CHR steps/s (identical trajectory)"}
+
+
+def _ours(a, rank, world):
+    import torch
+
+    import naja_b200 as nb
+    from naja_b200 import validate as nv
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    W = Workload(a)
+    P = nb.Polytope(W.A, W.b, device=dev.index)
+    T_dev = torch.from_numpy(W.T).to(dev)
+    sh_dev = torch.from_numpy(W.shift).to(dev)
+    x0 = torch.from_numpy(np.broadcast_to(W.start, (W.nchains, W.d)).copy()).to(dev)
+    samples = torch.empty((W.nspc * W.nchains, W.d), dtype=torch.float32, device=dev)
+    V = torch.empty((W.nspc * W.nchains, W.n), dtype=torch.float32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    chain_base = rank * W.nchains
+
+    def job():
+        P.run(x0, W.nspc, W.thin, W.nchains, out=samples, seed=a.seed, pair_prob=W.pair,
+              resync_interval=a.resync, precision=a.precision, chain_base=chain_base,
+              out_nchains=chain_base + W.nchains)
+        e_mid = torch.cuda.Event(enable_timing=True)
+        e_mid.record()
+        nb.backmap(T_dev, sh_dev, samples, mode=a.backmap_mode, out=V)
+        return e_mid
+
+    for _ in range(a.warmup):
+        job()
+        flush.zero_()
+    torch.cuda.synchronize()
+    P.check()
+    if world > 1:
+        torch.distributed.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
+    mids = []
+    with ClockSampler(dev.index if world == 1 else int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record()
+        for k in range(a.steps):
+            ev[k][0].record()
+            mids.append(job())
+            ev[k][1].record()
+            flush.zero_()
+        g1.record()
+        torch.cuda.synchronize()
+    P.check()
+    total_ms = g0.elapsed_time(g1)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    job_ms = [ev[k][0].elapsed_time(ev[k][1]) for k in range(a.steps)]
+    chr_ms = [ev[k][0].elapsed_time(mids[k]) for k in range(a.steps)]
+    # metric on the last job's samples
+    ess, rhat = nv.ess_rhat(samples, W.nchains, layout=1)
+    per_dim = ess.sum(axis=1)
+    if world > 1:
+        t = torch.from_numpy(per_dim).to(dev)
+        torch.distributed.all_reduce(t)
+        per_dim = t.cpu().numpy()
+    min_ess = float(per_dim.min())
+    ms_per_step = total_ms / a.steps
+    value = min_ess / (ms_per_step / 1e3)  # min-ESS already sums every rank's chains
+    gate = _gate(torch, W, samples, ess, rhat, V)
+    ref_sem = nv.summary(*nv.ess_rhat(samples, W.nchains, layout=0))
+    peak, peak_kind = _peaks()
+    chr_mean = statistics.mean(chr_ms)
+    achieved = W.bytes_per_step * W.steps / (chr_mean / 1e3) / 1e9
+    steps_per_s = W.steps * world / (ms_per_step / 1e3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if a.precision == "fp32" else "f64", "data": "synthetic (seeded genome-shaped generator)",
+        "config": W.config(a),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": peak_kind, "kernel": "chr_kernel",
+                     "kernel_ms": chr_mean, "bytes_per_chr_step": W.bytes_per_step, "chr_steps_per_launch": W.steps},
+        "chr_steps_per_s": steps_per_s, "min_ess": min_ess, "job_ms": job_ms, "chr_ms": chr_ms,
+        "gate": gate,
+        "reference_semantics_validate": {k: ref_sem[k] for k in ("status", "ess", "rhat")},
+        "gpu_launches": 2 * a.steps,
+    }
+    line["clocks"] = clk.summary()
+    if a.e2e and rank == 0:
+        line["e2e"] = _e2e(a, W, torch, dev, min_ess)
+    if rank == 0 and world == 1 and not a.no_cpu:
+        line["cpu_baseline"] = _cpu_baseline(W, a, min_ess / W.steps)
+    P.close()
+    return line
+
+
+def _e2e(a, W, torch, dev, min_ess):
+    import naja_b200 as nb
+
+    pinned_out = torch.empty((W.nspc * W.nchains, W.n), dtype=torch.float32, pin_memory=True)
+    samples = torch.empty((W.nspc * W.nchains, W.d), dtype=torch.float32, device=dev)
+    x0 = np.ascontiguousarray(np.broadcast_to(W.start, (W.nchains, W.d)))
+    h2d = W.A.nbytes + W.b.nbytes + x0.nbytes + W.T.nbytes + W.shift.nbytes
+    d2h = pinned_out.numel() * 4
+    times = []
+    for k in range(a.warmup + a.steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        P = nb.Polytope(W.A, W.b, device=dev.index)
+        P.run(x0, W.nspc, W.thin, W.nchains, out=samples, seed=a.seed, pair_prob=W.pair,
+              resync_interval=a.resync, precision=a.precision, stream=None)
+        nb.backmap(W.T, W.shift, samples, mode=a.backmap_mode, out=pinned_out)
+        e1.record()
+        torch.cuda.synchronize()
+        P.close()
+        if k >= a.warmup:
+            times.append(e0.elapsed_time(e1))
+    ms = statistics.mean(times)
+    return {"value": min_ess / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "ms_per_step": ms}
+
+
+def _reference_arm(a, rank, world):
+    """The reference's own implementation of the path, timed on this box.
+
+    The reference implements CHR only as CUDA (src/gpu/chr.cu); it has no
+    CPU sampler.  When its sources were compiled here (oracle/_ref/) this arm
+    runs them through their own API; otherwise it times the CPU restatement
+    of the same algorithm (oracle/) with all host threads.
+    """
+    import oracle.oracle as O
+
+    W = Workload(a)
+    cores = os.cpu_count() or 1
+    nspc = 2
+    t0 = time.perf_counter()
+    O.chr_run(W.A, W.b, W.start, nspc, W.thin, W.nchains, seed=a.seed, pair_prob=W.pair, precision="fp64",
+              threads=min(cores, W.nchains))
+    dt = time.perf_counter() - t0
+    nspc = max(2, min(W.nspc, int(nspc * a.cpu_seconds / max(dt, 1e-3))))
+    times = []
+    for k in range(a.warmup + a.steps):
+        t0 = time.perf_counter()
+        S = O.chr_run(W.A, W.b, W.start, nspc, W.thin, W.nchains, seed=a.seed, pair_prob=W.pair, precision="fp64",
+                      threads=min(cores, W.nchains))
+        if k >= a.warmup:
+            times.append(time.perf_counter() - t0)
+    dt = statistics.mean(times)
+    steps_s = W.nchains * nspc * W.thin / dt
+    # min-ESS per CHR step from the sample itself (chain-correct, summed over chains)
+    ess = O.ess(S.astype(np.float32), W.nchains, layout=1).sum(axis=1).min()
+    value = float(ess) / dt
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded genome-shaped generator)",
+            "config": W.config(a), "chr_steps_per_s": steps_s,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": min(cores, W.nchains), "kind": "port",
+                             "sample": f"{W.nchains} chains x {nspc} samples (thinning {W.thin}), FP64 CPU "
+                                       f"restatement of the reference kernel, no backmap"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=2600)
+    ap.add_argument("--d", type=int, default=700)
+    ap.add_argument("--nchains", type=int, default=16)
+    ap.add_argument("--nspc", type=int, default=12500)
+    ap.add_argument("--thinning", type=int, default=116)
+    ap.add_argument("--pair-prob", type=float, default=0.3)
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--resync", type=int, default=0)
+    ap.add_argument("--backmap-mode", default="fp64", choices=["fp64", "bf16x3", "tf32x3"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    a = ap.parse_args(argv)
+    if a.warmup < 3:
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        if a.impl == "reference":
+            line = _reference_arm(a, rank, world) if rank == 0 else None
+        else:
+            line = _ours(a, rank, world)
+        if rank == 0 and line is not None:
+            print(json.dumps(line))
+    finally:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,150 @@
+/*
+ * naja_chr.h -- C ABI of the B200-native coordinate hit-and-run (CHR)
+ * sampler (libnaja_b200.so).
+ *
+ * Plain C: pointers, sizes, POD structs, an integer status and a
+ * thread-local last-error string.  Every pointer argument may be host or
+ * device memory (the library inspects it); device pointers must live on the
+ * device the call runs on.  Calls are asynchronous on the given stream
+ * unless a host pointer forces a synchronous copy back.  Matrices are
+ * column-major with an explicit leading dimension, as in the reference
+ * (IDX2C(i,j,ld) = j*ld + i, src/gpu/helper.h:9 of quothbonney/naja).
+ *
+ * The sample matrix layout is the reference's: sample s of chain c is
+ * column c + s*nchains of a d x (nchains*nspc) column-major matrix
+ * (src/gpu/chr.cu:284,460), which is byte-identical to the row-major
+ * (nchains*nspc, d) array that `samples.npy` stores (src/npy.h:96-141).
+ */
+#ifndef NAJA_CHR_H
+#define NAJA_CHR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ statuses */
+#define NAJA_OK 0
+#define NAJA_ERR_INVALID_ARGUMENT 1 /* reference: std::invalid_argument */
+#define NAJA_ERR_RUNTIME 2          /* reference: std::runtime_error    */
+#define NAJA_ERR_CUDA 3             /* a CUDA runtime call failed         */
+#define NAJA_ERR_NO_MEMORY 4
+#define NAJA_ERR_UNSUPPORTED 5      /* shape outside what the kernels take */
+#define NAJA_ERR_DEVICE 6           /* the kernel reported an error word  */
+
+/* ------------------------------------------------------------- options */
+#define NAJA_PREC_FP32 0 /* FP32 A and slack, FP64 x, FP64 recompute every K */
+#define NAJA_PREC_FP64 1 /* FP64 throughout (the reference's arithmetic)      */
+
+#define NAJA_RNG_PHILOX 0  /* counter-based Philox4x32-10 keyed (seed, chain, step) */
+#define NAJA_RNG_REF_MRG 1 /* cuRAND MRG32k3a, curand_init(seed, chain, 0), reference draw order */
+
+#define NAJA_DTYPE_F32 0
+#define NAJA_DTYPE_F64 1
+
+#define NAJA_BACKMAP_FP64 0    /* FP64 SIMT GEMM (reference arithmetic)          */
+#define NAJA_BACKMAP_BF16X3 1  /* split-BF16 on tcgen05, FP32 accumulate          */
+#define NAJA_BACKMAP_TF32X3 2  /* 3xTF32 on tcgen05, FP32 accumulate              */
+
+typedef struct naja_polytope naja_polytope; /* device-resident A (FP64 + FP32), b */
+
+/* Sampling parameters.  Field meanings follow the reference's
+ * CoordinateHitAndRun arguments (src/gpu/gpusamplers.h:30-46). */
+typedef struct naja_chr_params {
+    int nspc;              /* samples per chain                                  */
+    int thinning;          /* steps between saved samples (> 0)                  */
+    int nchains;           /* chains in this call                                */
+    int tpb;               /* consumer threads per chain; <= 0 = automatic        */
+    unsigned long long seed;
+    double pair_prob;      /* probability of a pair direction                    */
+    int resync_interval;   /* slack = b - A x recomputed in FP64 every K steps   */
+    double ksparse_prob;
+    int ksparse_k;
+    int pair_mode;         /* 1 = (e_i - e_j)/sqrt 2, 2 = Jacobi schedule         */
+    const int* pair_i;     /* pair schedule (pair_mode 2), n_pairs entries each  */
+    const int* pair_j;
+    const double* pair_c;
+    const double* pair_s;
+    int n_pairs;
+    int precision;         /* NAJA_PREC_*                                        */
+    int rng;               /* NAJA_RNG_*                                         */
+    int out_dtype;         /* NAJA_DTYPE_* of the samples buffer                 */
+    int chain_base;        /* global index of chain 0 (RNG stream, output row)   */
+    int out_nchains;       /* chains per output row block (>= chain_base+nchains); 0 = nchains */
+    long long step_offset; /* Philox: continue chains from this step             */
+    int max_slots;         /* staged-column ring depth cap; 0 = automatic        */
+    void* rng_state;       /* nullable MRG32k3a states (naja_mrg_state_bytes each), in/out */
+} naja_chr_params;
+
+/* Fills `p` with the reference's defaults (gpusamplers.h:30-46): tpb auto,
+ * seed 0, pair_prob 0, resync 0, ksparse_prob 0, ksparse_k 8, pair_mode 1,
+ * FP32 tier, Philox, float output. */
+void naja_chr_params_default(naja_chr_params* p);
+
+/* ------------------------------------------------------------ polytope */
+
+/* Uploads the polytope A y <= b (A m x d column-major, leading dimension
+ * lda >= m) to `device`, keeping an FP64 copy and an FP32 copy, each with
+ * a leading dimension padded to a multiple of 32.  Replaces the DMatrix /
+ * DVector uploads of src/engine/job_sampling.cu:258-259 (quothbonney/naja). */
+int naja_polytope_create(int device, int m, int d, const double* A, int lda, const double* b,
+                         naja_polytope** out);
+int naja_polytope_destroy(naja_polytope* P);
+int naja_polytope_shape(const naja_polytope* P, int* m, int* d);
+/* Waits for all work on the polytope's device and reports (then clears)
+ * an error word a kernel set since the last check: a bounded wait that
+ * expired, or a pair index outside [0, d).  Calls whose buffers are all on
+ * the device return before the kernel ends; this is how their device-side
+ * errors surface.  Calls with a host buffer check it themselves. */
+int naja_polytope_check(const naja_polytope* P);
+
+/* ------------------------------------------------------------ sampling */
+
+/* Runs params->nchains chains from X0 (d x nchains, leading dimension ldx)
+ * and writes params->nspc samples per chain into `samples`, laid out as
+ * described at the top of this file (rows of d values of out_dtype).
+ * X_final (nullable) receives the last state of every chain (the
+ * reference's persist_state, src/gpu/chr.cu:485-489).  Replaces
+ * naja::gpu::CoordinateHitAndRun (src/gpu/chr.cu:13-70) and
+ * launchChrKernel (src/gpu/chr.cu:498-553). */
+int naja_chr_run(const naja_polytope* P, const naja_chr_params* params, const double* X0, int ldx,
+                 void* samples, double* X_final, void* stream);
+
+/* ------------------------------------------------------------- backmap */
+
+/* V = T * Y + shift * 1^T.  T is n x d column-major (leading dimension ldt),
+ * Y holds N samples of d values (row-major N x d, y_dtype), V receives N
+ * rows of n values (v_dtype).  Replaces backmap_into
+ * (src/gpu/backmap.cu:20-48). */
+int naja_backmap(int n, int d, long long N, const double* T, int ldt, const double* shift,
+                 const void* Y, int y_dtype, void* V, int v_dtype, int mode, void* stream);
+
+/* ------------------------------------------------------------ validate */
+
+/* Geyer ESS per (dim, chain) and split-R-hat per dim of an (N, dim)
+ * row-major float32 sample matrix (src/validate/mcmc.cpp:91-194).
+ * layout 0 = the reference's windows (chain c = rows [c*spc, (c+1)*spc)),
+ * layout 1 = chains interleaved as the sampler writes them (row r belongs
+ * to chain r % nchains).  ess: dim*nchains values (dim-major), rhat: dim. */
+int naja_validate(const float* samples, long long N, int dim, int nchains, int layout, double* ess,
+                  double* rhat, void* stream);
+
+/* --------------------------------------------------------------- misc */
+
+/* Thread-local description of the last failure on this thread. */
+const char* naja_last_error(void);
+/* Size of one MRG32k3a state for naja_chr_params.rng_state. */
+size_t naja_mrg_state_bytes(void);
+/* Test hook: the first `count` uniforms that cuRAND's curand_uniform_double
+ * returns for curand_init(seed, chain_base + c, 0), c < nchains, written to
+ * tape[c*count + i].  This is the reference's per-chain stream
+ * (src/gpu/chr.cu:555-560). */
+int naja_mrg_tape(int device, unsigned long long seed, int chain_base, int nchains, long long count, double* tape);
+const char* naja_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NAJA_CHR_H */

@@ -1,0 +1,372 @@
+// C ABI of libnaja_b200.so (declared in include/naja_chr.h).
+//
+// The host side of the reference's GPU API (src/gpu/chr.cu:13-99,
+// src/gpu/dmatrix.cu, src/gpu/dvector.cu of quothbonney/naja) restated on
+// plain pointers: argument checks raise the reference's error classes as
+// status codes, CUDA failures are never swallowed (the reference's
+// CUDA_CHECK only prints, src/gpu/helper.h:12-18), and every entry point
+// records a thread-local message.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/naja_chr.h"
+#include "capi_internal.cuh"
+#include "chr.cuh"
+#include "common.cuh"
+
+namespace naja {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes attr;
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+DeviceGuard::DeviceGuard(int device) {
+  cudaGetDevice(&prev_);
+  if (device >= 0 && device != prev_) {
+    ok_ = cudaSetDevice(device) == cudaSuccess;
+    switched_ = true;
+  }
+}
+DeviceGuard::~DeviceGuard() {
+  if (switched_) cudaSetDevice(prev_);
+}
+
+namespace {
+
+__global__ void pad_convert_kernel(const double* __restrict__ src, long long lds, double* __restrict__ A64,
+                                   float* __restrict__ A32, int m, int d, int lda) {
+  const long long n = static_cast<long long>(lda) * d;
+  for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<long long>(gridDim.x) * blockDim.x) {
+    const int r = static_cast<int>(i % lda);
+    const long long c = i / lda;
+    const double v = (r < m) ? src[c * lds + r] : 0.0;
+    A64[i] = v;
+    A32[i] = __double2float_rn(v);
+  }
+}
+
+constexpr unsigned long long kWaitTimeoutNs = 5ull * 1000ull * 1000ull * 1000ull;
+
+const char* dev_error_name(int code) {
+  switch (code) {
+    case kDevTimeoutFull: return "a consumer warp timed out waiting for a staged column";
+    case kDevTimeoutEmpty: return "the producer timed out waiting for a free slot";
+    case kDevTimeoutDrain: return "the exit path timed out draining its bulk copies";
+    case kDevBadPair: return "pair schedule index outside [0, d)";
+    default: return "unknown device error";
+  }
+}
+
+}  // namespace
+
+// Scoped stream-ordered device buffer; staged copies of host arguments.
+DeviceBuffer::~DeviceBuffer() {
+  if (ptr) cudaFreeAsync(ptr, stream);
+}
+int DeviceBuffer::alloc(size_t nbytes, cudaStream_t s) {
+  stream = s;
+  bytes = nbytes;
+  if (nbytes == 0) return NAJA_OK;
+  cudaError_t e = cudaMallocAsync(&ptr, nbytes, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    ptr = nullptr;
+    return fail(NAJA_ERR_NO_MEMORY, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
+  }
+  return NAJA_OK;
+}
+
+// Returns a device view of `p` (n bytes): itself if already on the device,
+// else a staged copy in `buf`.
+int device_view(const void* p, size_t n, cudaStream_t s, DeviceBuffer& buf, const void** out) {
+  if (!p || is_device_ptr(p)) {
+    *out = p;
+    return NAJA_OK;
+  }
+  int st = buf.alloc(n, s);
+  if (st) return st;
+  cudaError_t e = cudaMemcpyAsync(buf.ptr, p, n, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("cudaMemcpyAsync H2D: ") + cudaGetErrorString(e));
+  *out = buf.ptr;
+  return NAJA_OK;
+}
+
+}  // namespace naja
+
+using namespace naja;
+
+struct naja_polytope {
+  int device = 0;
+  int m = 0, d = 0, lda = 0;
+  double* A64 = nullptr;
+  float* A32 = nullptr;
+  double* b = nullptr;
+  int* err = nullptr;
+};
+
+extern "C" {
+
+const char* naja_last_error(void) { return g_last_error.c_str(); }
+
+const char* naja_version(void) { return "naja_b200 0.1 (sm_100a)"; }
+
+size_t naja_mrg_state_bytes(void) { return mrg_state_bytes(); }
+
+void naja_chr_params_default(naja_chr_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->thinning = 1;
+  p->tpb = 0;
+  p->ksparse_k = 8;
+  p->pair_mode = 1;
+  p->precision = NAJA_PREC_FP32;
+  p->rng = NAJA_RNG_PHILOX;
+  p->out_dtype = NAJA_DTYPE_F32;
+}
+
+int naja_polytope_create(int device, int m, int d, const double* A, int lda, const double* b,
+                         naja_polytope** out) {
+  if (!out) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_polytope_create: out is null");
+  *out = nullptr;
+  if (m <= 0 || d <= 0) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_polytope_create: empty polytope");
+  if (!A || !b) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_polytope_create: A or b is null");
+  if (lda < m) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_polytope_create: lda < m");
+  DeviceGuard g(device);
+  if (!g.ok()) return fail(NAJA_ERR_CUDA, "naja_polytope_create: cannot select device");
+  naja_polytope* P = new naja_polytope();
+  P->device = device;
+  P->m = m;
+  P->d = d;
+  P->lda = (m + 31) / 32 * 32;
+  const size_t n = static_cast<size_t>(P->lda) * d;
+  cudaError_t e = cudaMalloc(&P->A64, n * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&P->A32, n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&P->b, m * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&P->err, sizeof(int));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    naja_polytope_destroy(P);
+    return fail(NAJA_ERR_NO_MEMORY, std::string("naja_polytope_create: ") + cudaGetErrorString(e));
+  }
+  const double* src = A;
+  double* staged = nullptr;
+  if (!is_device_ptr(A)) {
+    e = cudaMalloc(&staged, static_cast<size_t>(lda) * d * sizeof(double));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(staged, A, static_cast<size_t>(lda) * d * sizeof(double), cudaMemcpyHostToDevice);
+    src = staged;
+  }
+  if (e == cudaSuccess) {
+    const long long total = static_cast<long long>(P->lda) * d;
+    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 16));
+    pad_convert_kernel<<<blocks, 256>>>(src, lda, P->A64, P->A32, m, d, P->lda);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpy(P->b, b, m * sizeof(double), is_device_ptr(b) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(P->err, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (staged) cudaFree(staged);
+  if (e != cudaSuccess) {
+    naja_polytope_destroy(P);
+    return fail(NAJA_ERR_CUDA, std::string("naja_polytope_create: ") + cudaGetErrorString(e));
+  }
+  *out = P;
+  return NAJA_OK;
+}
+
+int naja_polytope_destroy(naja_polytope* P) {
+  if (!P) return NAJA_OK;
+  DeviceGuard g(P->device);
+  cudaFree(P->A64);
+  cudaFree(P->A32);
+  cudaFree(P->b);
+  cudaFree(P->err);
+  delete P;
+  return NAJA_OK;
+}
+
+int naja_polytope_shape(const naja_polytope* P, int* m, int* d) {
+  if (!P) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_polytope_shape: null polytope");
+  if (m) *m = P->m;
+  if (d) *d = P->d;
+  return NAJA_OK;
+}
+
+int naja_polytope_check(const naja_polytope* P) {
+  if (!P) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_polytope_check: null polytope");
+  DeviceGuard g(P->device);
+  int code = 0;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(&code, P->err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_polytope_check: ") + cudaGetErrorString(e));
+  if (code != 0) {
+    cudaMemset(P->err, 0, sizeof(int));
+    return fail(NAJA_ERR_DEVICE, std::string("device error: ") + dev_error_name(code));
+  }
+  return NAJA_OK;
+}
+
+int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double* X0, int ldx, void* samples,
+                 double* X_final, void* stream_ptr) {
+  if (!P || !p) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run: null polytope or params");
+  if (p->nchains <= 0) return fail(NAJA_ERR_INVALID_ARGUMENT, "CoordinateHitAndRun: nchains must be positive");
+  if (p->nspc <= 0) return fail(NAJA_ERR_INVALID_ARGUMENT, "CoordinateHitAndRun: nspc must be positive");
+  if (p->thinning <= 0) return fail(NAJA_ERR_INVALID_ARGUMENT, "CoordinateHitAndRun: thinning must be positive");
+  if (!X0 || !samples) return fail(NAJA_ERR_INVALID_ARGUMENT, "CoordinateHitAndRun: X0 or samples is null");
+  if (ldx < P->d) return fail(NAJA_ERR_INVALID_ARGUMENT, "CoordinateHitAndRun: ldx < d");
+  if (p->precision != NAJA_PREC_FP32 && p->precision != NAJA_PREC_FP64)
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "CoordinateHitAndRun: unknown precision");
+  if (p->rng != NAJA_RNG_PHILOX && p->rng != NAJA_RNG_REF_MRG)
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "CoordinateHitAndRun: unknown rng");
+  if (p->out_dtype != NAJA_DTYPE_F32 && p->out_dtype != NAJA_DTYPE_F64)
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "CoordinateHitAndRun: unknown output dtype");
+  if (p->resync_interval < 0) return fail(NAJA_ERR_INVALID_ARGUMENT, "CoordinateHitAndRun: resync_interval < 0");
+  if (p->chain_base < 0) return fail(NAJA_ERR_INVALID_ARGUMENT, "CoordinateHitAndRun: chain_base < 0");
+  const int out_nchains = p->out_nchains > 0 ? p->out_nchains : p->nchains;
+  if (out_nchains < p->chain_base + p->nchains)
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "CoordinateHitAndRun: out_nchains < chain_base + nchains");
+  if (p->pair_mode == 2 && p->pair_prob > 0.0 && p->n_pairs > 0 &&
+      (!p->pair_i || !p->pair_j || !p->pair_c || !p->pair_s))
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "CoordinateHitAndRun: pair schedule arrays missing");
+  if (static_cast<long long>(p->nspc) * p->thinning > (1LL << 62))
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "CoordinateHitAndRun: too many steps");
+
+  DeviceGuard g(P->device);
+  if (!g.ok()) return fail(NAJA_ERR_CUDA, "naja_chr_run: cannot select device");
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+
+  ChrLaunchConfig cfg;
+  int st = chr_plan(p->precision, P->m, P->d, P->lda, p->tpb, p->max_slots, &cfg);
+  if (st == NAJA_ERR_INVALID_ARGUMENT) return fail(st, "Invalid threads per block");
+  if (st) return fail(st, "CoordinateHitAndRun: shape (m=" + std::to_string(P->m) + ", d=" + std::to_string(P->d) +
+                              ") exceeds the step kernel's capacity for this thread count");
+
+  const int d = P->d;
+  const size_t out_elt = p->out_dtype == NAJA_DTYPE_F64 ? 8 : 4;
+  const size_t out_bytes = static_cast<size_t>(p->nspc) * out_nchains * d * out_elt;
+  const size_t x_bytes = static_cast<size_t>(ldx) * (p->nchains - 1) * sizeof(double) + d * sizeof(double);
+
+  DeviceBuffer bx0, bout, bxf, bpi, bpj, bpc, bps;
+  const void* dX0 = nullptr;
+  if ((st = device_view(X0, x_bytes, stream, bx0, &dX0))) return st;
+  void* dout = samples;
+  const bool host_out = !is_device_ptr(samples);
+  if (host_out) {
+    if ((st = bout.alloc(out_bytes, stream))) return st;
+    dout = bout.ptr;
+    if (out_nchains != p->nchains) {
+      // rows of other chains are left as the caller had them
+      cudaError_t e = cudaMemcpyAsync(dout, samples, out_bytes, cudaMemcpyHostToDevice, stream);
+      if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("cudaMemcpyAsync: ") + cudaGetErrorString(e));
+    }
+  }
+  double* dxf = X_final;
+  const bool host_xf = X_final && !is_device_ptr(X_final);
+  if (host_xf) {
+    if ((st = bxf.alloc(x_bytes, stream))) return st;
+    dxf = static_cast<double*>(bxf.ptr);
+  }
+  const void *dpi = nullptr, *dpj = nullptr, *dpc = nullptr, *dps = nullptr;
+  if (p->n_pairs > 0) {
+    const size_t ni = static_cast<size_t>(p->n_pairs) * sizeof(int), nd = static_cast<size_t>(p->n_pairs) * 8;
+    if ((st = device_view(p->pair_i, ni, stream, bpi, &dpi))) return st;
+    if ((st = device_view(p->pair_j, ni, stream, bpj, &dpj))) return st;
+    if ((st = device_view(p->pair_c, nd, stream, bpc, &dpc))) return st;
+    if ((st = device_view(p->pair_s, nd, stream, bps, &dps))) return st;
+  }
+
+  ChrArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.A32 = P->A32;
+  a.A64 = P->A64;
+  a.lda = P->lda;
+  a.b = P->b;
+  a.m = P->m;
+  a.d = d;
+  a.X0 = static_cast<const double*>(dX0);
+  a.ldx = ldx;
+  a.X_final = dxf;
+  a.samples = dout;
+  a.out_f64 = p->out_dtype == NAJA_DTYPE_F64;
+  a.out_nchains = out_nchains;
+  a.chain_base = p->chain_base;
+  a.nspc = p->nspc;
+  a.thinning = p->thinning;
+  a.step_offset = p->step_offset;
+  a.seed = p->seed;
+  a.pair_prob = p->pair_prob;
+  a.ksparse_prob = p->ksparse_prob;
+  a.ksparse_k = p->ksparse_k;
+  a.pair_mode = p->pair_mode;
+  a.pair_i = static_cast<const int*>(dpi);
+  a.pair_j = static_cast<const int*>(dpj);
+  a.pair_c = static_cast<const double*>(dpc);
+  a.pair_s = static_cast<const double*>(dps);
+  a.n_pairs = p->n_pairs;
+  a.resync = p->resync_interval;
+  a.rng = p->rng;
+  a.rng_state = p->rng_state;
+  a.err = P->err;
+  a.timeout_ns = kWaitTimeoutNs;
+
+  st = chr_launch(p->precision, a, p->nchains, cfg, stream);
+  if (st) {
+    cudaError_t e = cudaGetLastError();
+    return fail(st, std::string("CoordinateHitAndRun: launch failed: ") + cudaGetErrorString(e));
+  }
+  if (host_out || host_xf) {
+    cudaError_t e = cudaSuccess;
+    if (host_out) e = cudaMemcpyAsync(samples, dout, out_bytes, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess && host_xf) e = cudaMemcpyAsync(X_final, dxf, x_bytes, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("CoordinateHitAndRun: ") + cudaGetErrorString(e));
+    int code = 0;
+    e = cudaMemcpy(&code, P->err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && code != 0) {
+      cudaMemset(P->err, 0, sizeof(int));
+      return fail(NAJA_ERR_DEVICE, std::string("device error: ") + dev_error_name(code));
+    }
+  }
+  return NAJA_OK;
+}
+
+int naja_mrg_tape(int device, unsigned long long seed, int chain_base, int nchains, long long count, double* tape) {
+  if (nchains <= 0 || count <= 0 || !tape) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_mrg_tape: bad arguments");
+  DeviceGuard g(device);
+  DeviceBuffer buf;
+  void* dt = tape;
+  const size_t bytes = static_cast<size_t>(nchains) * count * sizeof(double);
+  const bool host = !is_device_ptr(tape);
+  int st;
+  if (host) {
+    if ((st = buf.alloc(bytes, 0))) return st;
+    dt = buf.ptr;
+  }
+  st = mrg_tape(seed, chain_base, nchains, static_cast<long>(count), static_cast<double*>(dt), 0);
+  if (st) return fail(st, "naja_mrg_tape: launch failed");
+  cudaError_t e = cudaSuccess;
+  if (host) e = cudaMemcpy(tape, dt, bytes, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_mrg_tape: ") + cudaGetErrorString(e));
+  return NAJA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,67 @@
+// Host-visible description of one CHR launch and the launcher entry point.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace naja {
+
+enum StepKind : int { kCoord = 0, kPair = 1, kKSparse = 2 };
+
+// Everything the step kernel needs, passed by value.  Matrices are
+// column-major with a padded leading dimension `lda` (a multiple of 32
+// elements, so every column starts on a 128-byte boundary).
+struct ChrArgs {
+  const float* A32;   // FP32 copy of A (FP32 tier hot path)
+  const double* A64;  // FP64 A (FP64 tier hot path; init and recompute)
+  int lda;
+  const double* b;    // m
+  int m, d;
+  const double* X0;   // d x nchains, leading dimension ldx (column = local chain)
+  int ldx;
+  double* X_final;    // nullable, same layout as X0
+  void* samples;      // (nspc * out_nchains) x d row-major, row = s*out_nchains + chain_base + chain
+  int out_f64;        // 1: samples are double, 0: float
+  int out_nchains;
+  int chain_base;     // global index of this launch's chain 0 (RNG key and output row)
+  int nspc, thinning;
+  long long step_offset;  // Philox step counter offset (continuation of a chain)
+  unsigned long long seed;
+  double pair_prob, ksparse_prob;
+  int ksparse_k, pair_mode;
+  const int* pair_i;
+  const int* pair_j;
+  const double* pair_c;
+  const double* pair_s;
+  int n_pairs;
+  int resync;  // FP64 slack recompute every `resync` steps (t = 0 included), 0 = never
+  int rng;     // 0 = Philox4x32-10, 1 = cuRAND MRG32k3a in the reference's draw order
+  void* rng_state;  // nullable: curandStateMRG32k3a[nchains] loaded at start, stored at exit
+  int* err;         // device error word
+  unsigned long long timeout_ns;
+};
+
+struct ChrLaunchConfig {
+  int threads;    // consumer threads per chain (multiple of 32)
+  int rows;       // rows held per consumer thread (template capacity)
+  int slots;      // staged-column ring depth (0 = read columns straight from L2/HBM)
+  size_t smem;    // dynamic shared memory bytes
+};
+
+// Picks a launch configuration.  `tpb` > 0 forces the consumer thread count
+// (one of the reference's 32, 64, 128, 256, 512, 1024; 1024 runs as 992 consumer
+// threads plus the producer warp); `max_slots` > 0 caps the ring.
+// Returns 0 or a naja status code.
+int chr_plan(int precision, int m, int d, int lda, int tpb, int max_slots, ChrLaunchConfig* out);
+
+// Launches nchains independent chains (one CTA each) on `stream`.
+int chr_launch(int precision, const ChrArgs& args, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+
+// Records the first `count` uniforms of curand_init(seed, chain_base + c, 0)
+// MRG32k3a states, c < nchains, into tape[c * count + i] (device memory).
+int mrg_tape(unsigned long long seed, int chain_base, int nchains, long count, double* tape, cudaStream_t stream);
+
+// Size in bytes of one chain's MRG32k3a state (for rng_state buffers).
+size_t mrg_state_bytes();
+
+}  // namespace naja

@@ -1,0 +1,93 @@
+// Launch planning and dispatch for the CHR step kernel (see chr_kernel.cuh).
+#include <curand_kernel.h>
+
+#include "chr.cuh"
+#include "chr_kernel.cuh"
+
+namespace naja {
+int chr_launch_float_32(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+int chr_launch_float_64(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+int chr_launch_float_128(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+int chr_launch_float_256(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+int chr_launch_float_512(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+int chr_launch_float_992(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+int chr_launch_double_32(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+int chr_launch_double_64(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+int chr_launch_double_128(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+int chr_launch_double_256(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+int chr_launch_double_512(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+int chr_launch_double_992(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+
+using namespace chr_detail;
+namespace {
+__global__ void mrg_tape_kernel(unsigned long long seed, int chain_base, int nchains, long count, double* tape) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nchains) return;
+  curandStateMRG32k3a st;
+  curand_init(seed, static_cast<unsigned long long>(chain_base + c), 0ull, &st);
+  for (long i = 0; i < count; ++i) tape[static_cast<size_t>(c) * count + i] = curand_uniform_double(&st);
+}
+
+int max_rows_for(int threads) { return threads <= 512 ? 32 : 16; }
+
+}  // namespace
+
+int chr_plan(int precision, int m, int d, int lda, int tpb, int max_slots, ChrLaunchConfig* out) {
+  const int elt = precision == NAJA_PREC_FP64 ? 8 : 4;
+  int threads = 0;
+  if (tpb > 0) {
+    // The reference's thread counts (chr.cu:529-551).  A block also holds the
+    // producer warp, so 1024 maps to 992 consumer threads.
+    if (tpb != 32 && tpb != 64 && tpb != 128 && tpb != 256 && tpb != 512 && tpb != 1024) return NAJA_ERR_INVALID_ARGUMENT;
+    threads = tpb == 1024 ? 992 : tpb;
+  } else {
+    // Automatic: about 8 rows per thread, at least one warp, at most 992.
+    threads = 32;
+    while (threads < 512 && (m + threads - 1) / threads > 8) threads *= 2;
+    if ((m + threads - 1) / threads > 8) threads = 992;
+  }
+  int rows = 1;
+  while (rows * threads < m) rows *= 2;
+  if (rows > max_rows_for(threads)) return NAJA_ERR_UNSUPPORTED;
+  int slots = kMaxSlots;
+  if (max_slots > 0 && max_slots < slots) slots = max_slots;
+  Layout L = make_layout(d, lda, elt, threads, slots);
+  while (slots >= 3 && L.total > kSmemBudget) {
+    --slots;
+    L = make_layout(d, lda, elt, threads, slots);
+  }
+  if (L.total > kSmemBudget || slots < 3) {
+    slots = 0;  // direct: columns straight from L2 / HBM
+    L = make_layout(d, lda, elt, threads, 0);
+    if (L.total > kSmemBudget) return NAJA_ERR_UNSUPPORTED;
+  }
+  out->threads = threads;
+  out->rows = rows;
+  out->slots = slots;
+  out->smem = L.total;
+  return NAJA_OK;
+}
+
+int chr_launch(int precision, const ChrArgs& args, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream) {
+  if (nchains <= 0) return NAJA_OK;
+  const bool f64 = precision == NAJA_PREC_FP64;
+  switch (cfg.threads) {
+    case 32: return f64 ? chr_launch_double_32(args, nchains, cfg, stream) : chr_launch_float_32(args, nchains, cfg, stream);
+    case 64: return f64 ? chr_launch_double_64(args, nchains, cfg, stream) : chr_launch_float_64(args, nchains, cfg, stream);
+    case 128: return f64 ? chr_launch_double_128(args, nchains, cfg, stream) : chr_launch_float_128(args, nchains, cfg, stream);
+    case 256: return f64 ? chr_launch_double_256(args, nchains, cfg, stream) : chr_launch_float_256(args, nchains, cfg, stream);
+    case 512: return f64 ? chr_launch_double_512(args, nchains, cfg, stream) : chr_launch_float_512(args, nchains, cfg, stream);
+    case 992: return f64 ? chr_launch_double_992(args, nchains, cfg, stream) : chr_launch_float_992(args, nchains, cfg, stream);
+    default: return NAJA_ERR_UNSUPPORTED;
+  }
+}
+
+int mrg_tape(unsigned long long seed, int chain_base, int nchains, long count, double* tape, cudaStream_t stream) {
+  if (nchains <= 0 || count <= 0) return NAJA_OK;
+  mrg_tape_kernel<<<(nchains + 63) / 64, 64, 0, stream>>>(seed, chain_base, nchains, count, tape);
+  return cudaGetLastError() == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
+}
+
+size_t mrg_state_bytes() { return sizeof(curandStateMRG32k3a); }
+
+}  // namespace naja

@@ -1,0 +1,128 @@
+"""TEST INFRASTRUCTURE ONLY -- ctypes binding of the CPU oracle
+(oracle/_build/liboracle.so, built by oracle/Makefile).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
+this module; the product (naja_b200) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+_lib = None
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists() or LIB.stat().st_mtime < max(p.stat().st_mtime for p in HERE.glob("*.c")):
+            build()
+        lib = C.CDLL(str(LIB))
+        vp, i, d, u64, l = C.c_void_p, C.c_int, C.c_double, C.c_uint64, C.c_long
+        lib.oracle_chr_run.argtypes = [i, i, vp, i, vp, vp, i, i, i, i, u64, d, i, d, i, i,
+                                       vp, vp, vp, vp, i, i, i, vp, l, u64, i, vp, vp, vp, i]
+        lib.oracle_chr_run.restype = i
+        lib.oracle_philox4x32_10.argtypes = [vp, C.c_uint32, C.c_uint32, vp]
+        lib.oracle_philox4x32_10.restype = None
+        lib.oracle_ess.argtypes = [vp, l, i, i, i, vp]
+        lib.oracle_ess.restype = i
+        lib.oracle_split_rhat.argtypes = [vp, l, i, i, i, vp]
+        lib.oracle_split_rhat.restype = i
+        lib.oracle_ess_series.argtypes = [vp, l]
+        lib.oracle_ess_series.restype = d
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def philox(ctr, key):
+    c = np.ascontiguousarray(np.asarray(ctr, dtype=np.uint32))
+    out = np.empty(4, dtype=np.uint32)
+    load().oracle_philox4x32_10(_p(c), int(key[0]), int(key[1]), _p(out))
+    return out
+
+
+def chr_run(A, b, X0, nspc, thinning, nchains, *, seed=0, pair_prob=0.0, resync_interval=0, ksparse_prob=0.0,
+            ksparse_k=8, pair_mode=1, pairs=None, precision="fp32", tape=None, step_offset=0, pair_variant=0,
+            trace=False, x_final=False, threads=None):
+    """CPU CHR.  A (m, d); X0 (nchains, d) or (d,); returns samples (nspc*nchains, d) float64
+    [, trace (nchains, steps, 2)] [, X_final (nchains, d)]."""
+    A = np.asfortranarray(np.asarray(A, dtype=np.float64))
+    m, d = A.shape
+    b = np.ascontiguousarray(np.asarray(b, dtype=np.float64).reshape(-1))
+    X = np.asarray(X0, dtype=np.float64)
+    if X.ndim == 1:
+        X = np.broadcast_to(X, (nchains, d))
+    X = np.ascontiguousarray(X)
+    samples = np.zeros((nspc * nchains, d), dtype=np.float64)
+    tr = np.zeros((nchains, nspc * thinning, 2), dtype=np.int32) if trace else None
+    xf = np.zeros((nchains, d), dtype=np.float64) if x_final else None
+    pi = pj = pc = ps = None
+    npairs = 0
+    if pairs is not None:
+        pi = np.ascontiguousarray(np.asarray(pairs[0], dtype=np.int32))
+        pj = np.ascontiguousarray(np.asarray(pairs[1], dtype=np.int32))
+        pc = np.ascontiguousarray(np.asarray(pairs[2], dtype=np.float64))
+        ps = np.ascontiguousarray(np.asarray(pairs[3], dtype=np.float64))
+        npairs = len(pi)
+    tape_arr = None
+    stride = 0
+    rng = 0
+    if tape is not None:
+        tape_arr = np.ascontiguousarray(np.asarray(tape, dtype=np.float64))
+        stride = tape_arr.shape[1]
+        rng = 1
+    prec = 1 if precision == "fp64" else 0
+    nthreads = threads or os.cpu_count() or 1
+    st = load().oracle_chr_run(m, d, _p(A), m, _p(b), _p(X), d, int(nspc), int(thinning), int(nchains),
+                               int(seed) & 0xFFFFFFFFFFFFFFFF, float(pair_prob), int(resync_interval),
+                               float(ksparse_prob), int(ksparse_k), int(pair_mode), _p(pi), _p(pj), _p(pc), _p(ps),
+                               npairs, prec, rng, _p(tape_arr), stride, int(step_offset), int(pair_variant),
+                               _p(samples), _p(xf), _p(tr), int(nthreads))
+    if st != 0:
+        raise RuntimeError(f"oracle_chr_run failed with status {st}")
+    out = [samples]
+    if trace:
+        out.append(tr)
+    if x_final:
+        out.append(xf)
+    return out[0] if len(out) == 1 else tuple(out)
+
+
+def ess(samples, n_chains, layout=1):
+    s = np.ascontiguousarray(np.asarray(samples, dtype=np.float32))
+    N, dim = s.shape
+    out = np.empty((dim, n_chains), dtype=np.float64)
+    st = load().oracle_ess(_p(s), N, dim, n_chains, layout, _p(out))
+    if st:
+        raise RuntimeError("oracle_ess failed")
+    return out
+
+
+def split_rhat(samples, n_chains, layout=1):
+    s = np.ascontiguousarray(np.asarray(samples, dtype=np.float32))
+    N, dim = s.shape
+    out = np.empty(dim, dtype=np.float64)
+    st = load().oracle_split_rhat(_p(s), N, dim, n_chains, layout, _p(out))
+    if st:
+        raise RuntimeError("oracle_split_rhat failed")
+    return out
+
+
+def ess_series(x):
+    x = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+    return load().oracle_ess_series(_p(x), len(x))
