@@ -76,6 +76,8 @@ typedef struct naja_chr_params {
     long long step_offset; /* Philox: continue chains from this step             */
     int max_slots;         /* staged-column ring depth cap; 0 = automatic        */
     void* rng_state;       /* nullable MRG32k3a states (naja_mrg_state_bytes each), in/out */
+    unsigned long long* wait_cycles; /* nullable device buffer, 4 per chain: consumer wait for columns,
+                                        producer wait for slots, consumer loop, producer loop (SM cycles) */
 } naja_chr_params;
 
 /* Fills `p` with the reference's defaults (gpusamplers.h:30-46): tpb auto,
@@ -137,6 +139,12 @@ int naja_validate(const float* samples, long long N, int dim, int nchains, int l
 const char* naja_last_error(void);
 /* Size of one MRG32k3a state for naja_chr_params.rng_state. */
 size_t naja_mrg_state_bytes(void);
+/* Seeds `nchains` MRG32k3a states (device buffer, naja_mrg_state_bytes()
+ * each) with curand_init(seed, chain_base + c, 0), the reference's seeding
+ * (src/gpu/chr.cu:555-560).  A run given them in rng_state continues each
+ * stream and stores it back, as the reference's streamed mode carries its
+ * PRNGState across chunks (src/gpu/chr.cu:154-201). */
+int naja_mrg_init_states(int device, unsigned long long seed, int chain_base, int nchains, void* states);
 /* Test hook: the first `count` uniforms that cuRAND's curand_uniform_double
  * returns for curand_init(seed, chain_base + c, 0), c < nchains, written to
  * tape[c*count + i].  This is the reference's per-chain stream

@@ -41,6 +41,7 @@ EXPORTED = (
     "naja_last_error",
     "naja_mrg_state_bytes",
     "naja_mrg_tape",
+    "naja_mrg_init_states",
     "naja_version",
 )
 
@@ -72,6 +73,7 @@ class ChrParams(C.Structure):
         ("step_offset", C.c_longlong),
         ("max_slots", C.c_int),
         ("rng_state", C.c_void_p),
+        ("wait_cycles", C.c_void_p),
     ]
 
 
@@ -114,12 +116,13 @@ def load() -> C.CDLL:
     lib.naja_last_error.argtypes = []
     lib.naja_mrg_state_bytes.restype = C.c_size_t
     lib.naja_mrg_tape.argtypes = [i, ull, i, i, ll, vp]
+    lib.naja_mrg_init_states.argtypes = [i, ull, i, i, vp]
     lib.naja_version.restype = C.c_char_p
     for name in EXPORTED:
         f = getattr(lib, name)
         if f.restype is C.c_int or name in ("naja_polytope_create", "naja_polytope_destroy", "naja_polytope_shape",
                                                "naja_polytope_check", "naja_chr_run", "naja_backmap",
-                                               "naja_validate", "naja_mrg_tape"):
+                                               "naja_validate", "naja_mrg_tape", "naja_mrg_init_states"):
             f.restype = C.c_int
     _lib = lib
     return lib

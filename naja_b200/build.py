@@ -8,6 +8,7 @@ csrc/ or include/ is newer.  Usage: python -m naja_b200.build [-j N] [--clean]
 from __future__ import annotations
 
 import argparse
+import hashlib
 import os
 import shutil
 import subprocess
@@ -43,23 +44,31 @@ def _units():
     return units
 
 
-def _headers_mtime() -> float:
-    hs = list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h"))
-    return max((h.stat().st_mtime for h in hs), default=0.0)
+def _inputs_digest(src: Path, cmd: list[str]) -> str:
+    """Hash of the unit's source, every header it may include and its command.
+
+    Content hashes, not mtimes: an edit made while another build is still
+    compiling the old text must not be mistaken for up to date."""
+    h = hashlib.sha256(" ".join(cmd).encode())
+    for p in [src, *sorted(CSRC.glob("*.cuh")), *sorted((ROOT / "include").glob("*.h"))]:
+        h.update(p.name.encode())
+        h.update(p.read_bytes())
+    return h.hexdigest()
 
 
 def _compile(name, src, flags, force, verbose):
     obj = OUT / f"{name}.o"
-    if not force and obj.exists():
-        newest = max(src.stat().st_mtime, _headers_mtime(), Path(__file__).stat().st_mtime)
-        if obj.stat().st_mtime >= newest:
-            return obj, None
+    stamp = OUT / f"{name}.sha256"
     cmd = [NVCC, *ARCH, *BASE, *flags, "-c", str(src), "-o", str(obj)]
+    digest = _inputs_digest(src, cmd)
+    if not force and obj.exists() and stamp.exists() and stamp.read_text() == digest:
+        return obj, None
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         return obj, f"{' '.join(cmd)}\n{r.stdout}{r.stderr}"
+    stamp.write_text(digest)
     return obj, None
 
 
@@ -73,13 +82,18 @@ def build(jobs: int | None = None, force: bool = False, verbose: bool = False) -
     if errors:
         raise RuntimeError("nvcc failed:\n" + "\n\n".join(errors))
     objs = [o for o, _ in results]
-    if force or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+    link_stamp = OUT / "link.sha256"
+    h = hashlib.sha256()
+    for o in objs:
+        h.update(o.read_bytes())
+    if force or not LIB.exists() or not link_stamp.exists() or link_stamp.read_text() != h.hexdigest():
         tmp = LIB.with_suffix(".so.tmp")
         cmd = [NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(tmp), *map(str, objs)]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}{r.stderr}")
         os.replace(tmp, LIB)
+        link_stamp.write_text(h.hexdigest())
     return LIB
 
 

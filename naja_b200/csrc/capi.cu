@@ -74,6 +74,17 @@ const char* dev_error_name(int code) {
   }
 }
 
+// Reads (and clears) the error word of a finished launch.
+int read_device_error(int* err) {
+  int w[4] = {0, 0, 0, 0};
+  cudaError_t e = cudaMemcpy(w, err, sizeof(w), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("reading the device error word: ") + cudaGetErrorString(e));
+  if (w[0] == 0) return NAJA_OK;
+  cudaMemset(err, 0, sizeof(w));
+  return fail(NAJA_ERR_DEVICE, std::string("device error: ") + dev_error_name(w[0]) + " (" + std::to_string(w[1]) +
+                                   ", " + std::to_string(w[2]) + ", " + std::to_string(w[3]) + ")");
+}
+
 }  // namespace
 
 // Scoped stream-ordered device buffer; staged copies of host arguments.
@@ -159,7 +170,7 @@ int naja_polytope_create(int device, int m, int d, const double* A, int lda, con
   cudaError_t e = cudaMalloc(&P->A64, n * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&P->A32, n * sizeof(float));
   if (e == cudaSuccess) e = cudaMalloc(&P->b, m * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&P->err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&P->err, 4 * sizeof(int));
   if (e != cudaSuccess) {
     cudaGetLastError();
     naja_polytope_destroy(P);
@@ -181,7 +192,7 @@ int naja_polytope_create(int device, int m, int d, const double* A, int lda, con
   }
   if (e == cudaSuccess)
     e = cudaMemcpy(P->b, b, m * sizeof(double), is_device_ptr(b) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemset(P->err, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(P->err, 0, 4 * sizeof(int));
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (staged) cudaFree(staged);
   if (e != cudaSuccess) {
@@ -213,15 +224,9 @@ int naja_polytope_shape(const naja_polytope* P, int* m, int* d) {
 int naja_polytope_check(const naja_polytope* P) {
   if (!P) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_polytope_check: null polytope");
   DeviceGuard g(P->device);
-  int code = 0;
   cudaError_t e = cudaDeviceSynchronize();
-  if (e == cudaSuccess) e = cudaMemcpy(&code, P->err, sizeof(int), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_polytope_check: ") + cudaGetErrorString(e));
-  if (code != 0) {
-    cudaMemset(P->err, 0, sizeof(int));
-    return fail(NAJA_ERR_DEVICE, std::string("device error: ") + dev_error_name(code));
-  }
-  return NAJA_OK;
+  return read_device_error(P->err);
 }
 
 int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double* X0, int ldx, void* samples,
@@ -326,6 +331,7 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
   a.rng_state = p->rng_state;
   a.err = P->err;
   a.timeout_ns = kWaitTimeoutNs;
+  a.wait_cycles = p->wait_cycles;
 
   st = chr_launch(p->precision, a, p->nchains, cfg, stream);
   if (st) {
@@ -338,13 +344,19 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
     if (e == cudaSuccess && host_xf) e = cudaMemcpyAsync(X_final, dxf, x_bytes, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("CoordinateHitAndRun: ") + cudaGetErrorString(e));
-    int code = 0;
-    e = cudaMemcpy(&code, P->err, sizeof(int), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && code != 0) {
-      cudaMemset(P->err, 0, sizeof(int));
-      return fail(NAJA_ERR_DEVICE, std::string("device error: ") + dev_error_name(code));
-    }
+    if ((st = read_device_error(P->err))) return st;
   }
+  return NAJA_OK;
+}
+
+int naja_mrg_init_states(int device, unsigned long long seed, int chain_base, int nchains, void* states) {
+  if (nchains <= 0 || !states) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_mrg_init_states: bad arguments");
+  if (!is_device_ptr(states)) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_mrg_init_states: states must be device memory");
+  DeviceGuard g(device);
+  int st = mrg_init_states(seed, chain_base, nchains, states, 0);
+  if (st) return fail(st, "naja_mrg_init_states: launch failed");
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_mrg_init_states: ") + cudaGetErrorString(e));
   return NAJA_OK;
 }
 

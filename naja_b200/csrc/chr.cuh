@@ -39,6 +39,10 @@ struct ChrArgs {
   void* rng_state;  // nullable: curandStateMRG32k3a[nchains] loaded at start, stored at exit
   int* err;         // device error word
   unsigned long long timeout_ns;
+  // Nullable instrumentation, 4 words per chain: consumer cycles waiting for
+  // staged columns, producer cycles waiting for free slots, consumer cycles
+  // in the step loop, producer cycles in its loop.
+  unsigned long long* wait_cycles;
 };
 
 struct ChrLaunchConfig {
@@ -60,6 +64,9 @@ int chr_launch(int precision, const ChrArgs& args, int nchains, const ChrLaunchC
 // Records the first `count` uniforms of curand_init(seed, chain_base + c, 0)
 // MRG32k3a states, c < nchains, into tape[c * count + i] (device memory).
 int mrg_tape(unsigned long long seed, int chain_base, int nchains, long count, double* tape, cudaStream_t stream);
+
+// Seeds nchains MRG32k3a states with curand_init(seed, chain_base + c, 0).
+int mrg_init_states(unsigned long long seed, int chain_base, int nchains, void* states, cudaStream_t stream);
 
 // Size in bytes of one chain's MRG32k3a state (for rng_state buffers).
 size_t mrg_state_bytes();

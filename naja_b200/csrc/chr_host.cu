@@ -28,6 +28,11 @@ __global__ void mrg_tape_kernel(unsigned long long seed, int chain_base, int nch
   for (long i = 0; i < count; ++i) tape[static_cast<size_t>(c) * count + i] = curand_uniform_double(&st);
 }
 
+__global__ void mrg_init_kernel(unsigned long long seed, int chain_base, int nchains, curandStateMRG32k3a* st) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < nchains) curand_init(seed, static_cast<unsigned long long>(chain_base + c), 0ull, &st[c]);
+}
+
 int max_rows_for(int threads) { return threads <= 512 ? 32 : 16; }
 
 }  // namespace
@@ -85,6 +90,13 @@ int chr_launch(int precision, const ChrArgs& args, int nchains, const ChrLaunchC
 int mrg_tape(unsigned long long seed, int chain_base, int nchains, long count, double* tape, cudaStream_t stream) {
   if (nchains <= 0 || count <= 0) return NAJA_OK;
   mrg_tape_kernel<<<(nchains + 63) / 64, 64, 0, stream>>>(seed, chain_base, nchains, count, tape);
+  return cudaGetLastError() == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
+}
+
+int mrg_init_states(unsigned long long seed, int chain_base, int nchains, void* states, cudaStream_t stream) {
+  if (nchains <= 0) return NAJA_OK;
+  mrg_init_kernel<<<(nchains + 63) / 64, 64, 0, stream>>>(seed, chain_base, nchains,
+                                                         static_cast<curandStateMRG32k3a*>(states));
   return cudaGetLastError() == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
 }
 

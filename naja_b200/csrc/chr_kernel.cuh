@@ -57,6 +57,18 @@ struct __align__(16) StepMeta {
   double ks_coef[32];
 };
 
+// One step's direction as the producer draws it (register-resident; the
+// k-sparse index/coefficient lists live in small local arrays).
+struct StepDir {
+  int kind;
+  int ei;
+  int ej;
+  int k;
+  double ci;
+  double cj;
+  double u;
+};
+
 struct RedEntry {
   unsigned long long kmax;
   unsigned long long kmin;
@@ -135,7 +147,7 @@ struct MrgSource {
 // Draws one step's direction in the reference's order (chr.cu:285-364),
 // then the alpha uniform (chr.cu:437).  Returns false on a bad pair index.
 template <class Src>
-__device__ bool draw_direction(Src& src, const ChrArgs& a, StepMeta& o) {
+__device__ bool draw_direction(Src& src, const ChrArgs& a, StepDir& o, int* ks_idx, double* ks_coef) {
   const int cols = a.d;
   const double ucoord = src.next();
   const int want_ks = (a.ksparse_prob > 0.0 && ucoord < a.ksparse_prob) ? 1 : 0;
@@ -156,8 +168,8 @@ __device__ bool draw_direction(Src& src, const ChrArgs& a, StepMeta& o) {
       int idx = static_cast<int>(src.next() * static_cast<double>(cols));
       if (idx >= cols) idx = cols - 1;
       const double sign = (src.next() < 0.5) ? 1.0 : -1.0;
-      o.ks_idx[t] = idx;
-      o.ks_coef[t] = __dmul_rn(sign, inv_sqrt_k);
+      ks_idx[t] = idx;
+      ks_coef[t] = __dmul_rn(sign, inv_sqrt_k);
     }
   }
   bool ok = true;
@@ -219,19 +231,24 @@ struct Tier<float> {
   __device__ static float lowest() { return -3.402823466e+38f; }
   __device__ static float highest() { return 3.402823466e+38f; }
   __device__ static const float* A(const ChrArgs& a) { return a.A32; }
-  __device__ static float pair_ae(float ai, float aj, double ci, double cj) {
-    return __fmaf_rn(ai, static_cast<float>(ci), __fmul_rn(aj, static_cast<float>(cj)));
+  __device__ static float pair_ae_r(float ai, float aj, float ci, float cj) {
+    return __fmaf_rn(ai, ci, __fmul_rn(aj, cj));
   }
   __device__ static float ks_acc(float acc, float av, double coef) {
     return __fmaf_rn(av, static_cast<float>(coef), acc);
   }
   // Ratio ae/s with the reference's special cases; a negative FP32 slack
   // counts as 0 (it can only come from FP32 rounding).
+  // With s clamped to +0 the IEEE quotient is already the reference's
+  // s == 0 rule (ae/+0 = +-inf, 0/0 = NaN -> 0), so no branch is needed.
+  // A zero numerator is answered without dividing (the IEEE result: +-0 for
+  // s > 0, NaN -> 0 for s = +0): most rows of a sparse A are zero and a
+  // division of zero leaves the division's fast path.
   __device__ static float ratio(float ae, float s) {
-    if (s < 0.0f) s = 0.0f;
-    if (s == 0.0f) return ae > 0.0f ? __int_as_float(0x7f800000) : (ae < 0.0f ? __int_as_float(0xff800000) : 0.0f);
-    const float r = __fdiv_rn(ae, s);
-    return isnan(r) ? 0.0f : r;
+    s = (s <= 0.0f) ? 0.0f : s;
+    const bool z = (ae == 0.0f);
+    const float q = __fdiv_rn(z ? 1.0f : ae, z ? 1.0f : s);
+    return z ? ((s > 0.0f) ? ae : 0.0f) : ((q != q) ? 0.0f : q);
   }
   __device__ static float alpha(float mx, float mn, double u) {
     const float lo = __fdiv_rn(1.0f, mn), hi = __fdiv_rn(1.0f, mx);
@@ -266,16 +283,17 @@ struct Tier<double> {
   __device__ static double lowest() { return -1.7976931348623157e+308; }
   __device__ static double highest() { return 1.7976931348623157e+308; }
   __device__ static const double* A(const ChrArgs& a) { return a.A64; }
-  __device__ static double pair_ae(double ai, double aj, double ci, double cj) {
+  __device__ static double pair_ae_r(double ai, double aj, double ci, double cj) {
     return __fma_rn(ai, ci, __dmul_rn(aj, cj));
   }
   __device__ static double ks_acc(double acc, double av, double coef) { return __fma_rn(av, coef, acc); }
+  // s == 0 of either sign becomes +0: ae/+0 = +-inf, 0/0 = NaN -> 0, the
+  // reference's rule (chr.cu:420-429); negative slack divides as it is.
   __device__ static double ratio(double ae, double s) {
-    if (s == 0.0)
-      return ae > 0.0 ? __longlong_as_double(0x7ff0000000000000ll)
-                      : (ae < 0.0 ? __longlong_as_double(static_cast<long long>(0xfff0000000000000ull)) : 0.0);
-    const double r = __ddiv_rn(ae, s);
-    return isnan(r) ? 0.0 : r;
+    s = (s == 0.0) ? 0.0 : s;
+    const bool z = (ae == 0.0);
+    const double q = __ddiv_rn(z ? 1.0 : ae, z ? 1.0 : s);
+    return z ? ((s > 0.0) ? ae : ((s < 0.0) ? -ae : 0.0)) : ((q != q) ? 0.0 : q);
   }
   __device__ static double alpha(double mx, double mn, double u) {
     const double lo = __ddiv_rn(1.0, mn), hi = __ddiv_rn(1.0, mx);
@@ -301,38 +319,53 @@ __device__ __noinline__ void run_producer(const ChrArgs& a, Src& src, const Layo
   const uint32_t col_bytes = static_cast<uint32_t>(align_up(static_cast<size_t>(a.m) * sizeof(Real), 16));
   const int S = L.slots;
   const long long total = static_cast<long long>(a.nspc) * a.thinning;
-  uint64_t g = 0;
-  uint64_t last_use[kMaxSlots];
-  bool used[kMaxSlots];
-  for (int s = 0; s < kMaxSlots; ++s) used[s] = false;
-  StepMeta dir;
+  // Slots are claimed round-robin.  `slot` is the next one, `round` how many
+  // times the ring has wrapped: a slot's use number is the round it is
+  // claimed in, its fill waits for the empty-barrier phase of round - 1.
+  int slot = 0;
+  uint32_t round = 0;
+  uint32_t used_mask = 0, last_parity = 0;  // per slot: used at all / parity of its last use
+  StepDir dir;
+  int ks_idx[32];
+  double ks_coef[32];
+  unsigned long long w_empty = 0;
+  const unsigned long long p_start = clock64();
   for (long long t = 0; t < total; ++t) {
     if (*abort_flag) break;
     src.begin_step(static_cast<uint64_t>(a.step_offset + t));
-    if (!draw_direction(src, a, dir)) {
-      set_error(a.err, kDevBadPair);
+    if (!draw_direction(src, a, dir, ks_idx, ks_coef)) {
+      set_error(a.err, kDevBadPair, dir.ei, dir.ej, static_cast<int>(t));
       *abort_flag = 1;
       break;
     }
-    const int sa = static_cast<int>(g % S);
-    const uint64_t ua = g / S;
-    if (ua >= 1 && !mbar_wait_bounded(&empty[sa], static_cast<uint32_t>((ua - 1) & 1), a.timeout_ns)) {
-      set_error(a.err, kDevTimeoutEmpty);
+    const int sa = slot;
+    const uint32_t ra = round;
+    if (++slot == S) {
+      slot = 0;
+      ++round;
+    }
+    const unsigned long long w0 = a.wait_cycles ? clock64() : 0ull;
+    if (ra >= 1 && !mbar_wait_bounded(&empty[sa], (ra - 1) & 1u, a.timeout_ns)) {
+      set_error(a.err, kDevTimeoutEmpty, sa, static_cast<int>(ra), static_cast<int>(t));
       *abort_flag = 1;
       break;
     }
+    if (a.wait_cycles) w_empty += clock64() - w0;
     int sb = -1;
-    uint64_t ub = 0;
+    uint32_t rb = 0;
     if (dir.kind == kPair) {
-      sb = static_cast<int>((g + 1) % S);
-      ub = (g + 1) / S;
-      if (ub >= 1 && !mbar_wait_bounded(&empty[sb], static_cast<uint32_t>((ub - 1) & 1), a.timeout_ns)) {
-        set_error(a.err, kDevTimeoutEmpty);
+      sb = slot;
+      rb = round;
+      if (++slot == S) {
+        slot = 0;
+        ++round;
+      }
+      if (rb >= 1 && !mbar_wait_bounded(&empty[sb], (rb - 1) & 1u, a.timeout_ns)) {
+        set_error(a.err, kDevTimeoutEmpty, sb, static_cast<int>(rb), static_cast<int>(t));
         *abort_flag = 1;
         break;
       }
     }
-    g += (sb >= 0) ? 2 : 1;
     StepMeta& M = meta[sa];
     M.kind = dir.kind;
     M.ei = dir.ei;
@@ -344,19 +377,23 @@ __device__ __noinline__ void run_producer(const ChrArgs& a, Src& src, const Layo
     M.k = dir.k;
     if (dir.kind == kKSparse) {
       for (int q = 0; q < dir.k; ++q) {
-        M.ks_idx[q] = dir.ks_idx[q];
-        M.ks_coef[q] = dir.ks_coef[q];
+        M.ks_idx[q] = ks_idx[q];
+        M.ks_coef[q] = ks_coef[q];
       }
     }
+    // The drain below waits for the full-barrier phase of each slot's most
+    // recent use, whatever its kind, so every use is recorded here.
+    used_mask |= 1u << sa;
+    last_parity = (last_parity & ~(1u << sa)) | ((ra & 1u) << sa);
+    if (sb >= 0) {
+      used_mask |= 1u << sb;
+      last_parity = (last_parity & ~(1u << sb)) | ((rb & 1u) << sb);
+    }
     if (!L.direct && dir.kind != kKSparse) {
-      used[sa] = true;
-      last_use[sa] = ua;
       mbar_arrive_expect_tx(&full[sa], col_bytes);
       bulk_g2s(smem + L.slot_off + static_cast<size_t>(sa) * L.slot_bytes, A + static_cast<size_t>(dir.ei) * a.lda,
                col_bytes, &full[sa]);
       if (sb >= 0) {
-        used[sb] = true;
-        last_use[sb] = ub;
         mbar_arrive_expect_tx(&full[sb], col_bytes);
         bulk_g2s(smem + L.slot_off + static_cast<size_t>(sb) * L.slot_bytes,
                  A + static_cast<size_t>(dir.ej) * a.lda, col_bytes, &full[sb]);
@@ -366,10 +403,14 @@ __device__ __noinline__ void run_producer(const ChrArgs& a, Src& src, const Layo
       if (sb >= 0) mbar_arrive(&full[sb]);
     }
   }
+  if (a.wait_cycles) {
+    a.wait_cycles[4 * (blockIdx.x) + 1] = w_empty;
+    a.wait_cycles[4 * (blockIdx.x) + 3] = clock64() - p_start;
+  }
   // Drain: never leave the CTA with a bulk copy still writing into it.
-  for (int s = 0; s < S; ++s) {
-    if (used[s] && !mbar_wait_bounded(&full[s], static_cast<uint32_t>(last_use[s] & 1), a.timeout_ns)) {
-      set_error(a.err, kDevTimeoutDrain);
+  for (int q = 0; q < S; ++q) {
+    if (((used_mask >> q) & 1u) && !mbar_wait_bounded(&full[q], (last_parity >> q) & 1u, a.timeout_ns)) {
+      set_error(a.err, kDevTimeoutDrain, q, static_cast<int>((last_parity >> q) & 1u), static_cast<int>(round));
     }
   }
 }
@@ -434,10 +475,19 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
   recompute();
 
   const long long total = static_cast<long long>(a.nspc) * a.thinning;
-  uint64_t g = 0;
+  // Ring position (mirrors the producer), phase parity of the slot's fill,
+  // and step counters that replace t % thinning, t / thinning, t % resync.
+  int slot = 0;
+  uint32_t parity = 0;
+  int thin_ctr = 0, resync_ctr = 0, rbuf = 0;
+  size_t out_row = static_cast<size_t>(gchain);
+  unsigned long long w_full = 0;
+  const unsigned long long c_start = clock64();
   for (long long t = 0; t < total; ++t) {
-    const int sa = static_cast<int>(g % S);
-    bool ok = mbar_wait_bounded(&full[sa], static_cast<uint32_t>((g / S) & 1), a.timeout_ns);
+    const int sa = slot;
+    const unsigned long long w0 = a.wait_cycles ? clock64() : 0ull;
+    bool ok = mbar_wait_bounded(&full[sa], parity, a.timeout_ns);
+    if (a.wait_cycles) w_full += clock64() - w0;
     int kind = kCoord, ei = 0, ej = 0, sb = -1, kq = 0;
     double ci = 1.0, cj = 0.0, u = 0.5;
     if (ok) {
@@ -450,53 +500,74 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
       cj = M.cj;
       u = M.u;
       kq = M.k;
-      ++g;
+      if (++slot == S) {
+        slot = 0;
+        parity ^= 1u;
+      }
       if (kind == kPair) {
-        ok = mbar_wait_bounded(&full[sb], static_cast<uint32_t>((g / S) & 1), a.timeout_ns);
-        ++g;
+        ok = mbar_wait_bounded(&full[sb], parity, a.timeout_ns);
+        if (++slot == S) {
+          slot = 0;
+          parity ^= 1u;
+        }
       }
     }
     // Uniform across every consumer warp (a named barrier follows), whatever `ok` is.
-    if (a.resync > 0 && (t % a.resync) == 0) {
-      named_bar_sync(2, NT);  // every owner's x update of step t-1 is visible
-      recompute();
+    if (a.resync > 0) {
+      if (resync_ctr == 0) {
+        named_bar_sync(2, NT);  // every owner's x update of the previous step is visible
+        recompute();
+      }
+      if (++resync_ctr == a.resync) resync_ctr = 0;
     }
     Key kmax = T::key(T::lowest()), kmin = T::key(T::highest());
-    // Column(s) of this step: staged in the ring, or straight from L2/HBM.
-    const Real* ca = L.direct ? A + static_cast<size_t>(ei) * lda
-                              : reinterpret_cast<const Real*>(smem + L.slot_off + static_cast<size_t>(sa) * L.slot_bytes);
-    const Real* cb = (kind == kPair)
-                         ? (L.direct ? A + static_cast<size_t>(ej) * lda
-                                     : reinterpret_cast<const Real*>(smem + L.slot_off +
-                                                                     static_cast<size_t>(sb) * L.slot_bytes))
-                         : ca;
-    // ae = A u for row r; evaluated identically in the ratio pass and the
+    // Row passes, specialised once per step on the (warp-uniform) kind and
+    // on where the column lives, so the per-row code is straight-line.
+    // ae = A u for row r is evaluated identically in the ratio pass and the
     // slack update (the slot stays resident until the step releases it).
-    auto ae_of = [&](int r) -> Real {
-      if (kind == kCoord) return ca[r];
-      if (kind == kPair) return T::pair_ae(ca[r], cb[r], ci, cj);
+    auto scan = [&](auto ae_at) {
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        const int r = tid + k * NT;
+        if (r < m) {
+          const Key kv = T::key(T::ratio(ae_at(r), sl[k]));
+          kmax = kv > kmax ? kv : kmax;
+          kmin = kv < kmin ? kv : kmin;
+        }
+      }
+    };
+    const Real cir = static_cast<Real>(ci), cjr = static_cast<Real>(cj);
+    const Real* gca = A + static_cast<size_t>(ei) * lda;
+    const Real* gcb = A + static_cast<size_t>(ej) * lda;
+    const Real* sca = reinterpret_cast<const Real*>(smem + L.slot_off + static_cast<size_t>(sa) * L.slot_bytes);
+    const Real* scb = reinterpret_cast<const Real*>(smem + L.slot_off +
+                                                    static_cast<size_t>(sb < 0 ? 0 : sb) * L.slot_bytes);
+    auto ks_at = [&](int r) -> Real {
       const StepMeta& M = meta[sa];
       Real acc = Real(0);
       for (int q = 0; q < kq; ++q) acc = T::ks_acc(acc, A[r + static_cast<size_t>(M.ks_idx[q]) * lda], M.ks_coef[q]);
       return acc;
     };
-    if (ok) {
-#pragma unroll
-      for (int k = 0; k < R; ++k) {
-        const int r = tid + k * NT;
-        if (r < m) {
-          const Real v = ae_of(r);
-          const Key kv = T::key(T::ratio(v, sl[k]));
-          kmax = kv > kmax ? kv : kmax;
-          kmin = kv < kmin ? kv : kmin;
-        }
+    auto for_kind = [&](auto pass) {
+      if (kind == kCoord) {
+        if (L.direct) pass([&](int r) -> Real { return gca[r]; });
+        else pass([&](int r) -> Real { return sca[r]; });
+      } else if (kind == kPair) {
+        if (L.direct) pass([&](int r) -> Real { return T::pair_ae_r(gca[r], gcb[r], cir, cjr); });
+        else pass([&](int r) -> Real { return T::pair_ae_r(sca[r], scb[r], cir, cjr); });
+      } else {
+        pass(ks_at);
       }
-    }
+    };
+    if (ok) for_kind([&](auto ae_at) { scan(ae_at); });
     kmax = T::wmax(kmax);
     kmin = T::wmin(kmin);
-    Real mx = T::unkey(kmax), mn = T::unkey(kmin);
     if (NW > 1) {
-      RedEntry* slotr = red + (t & 1) * NW;
+      // Lane 0 of each warp posts its warp's extremes; after one barrier lane
+      // l of every warp picks up warp l's entry and a second warp reduction
+      // yields the block's.  Double-buffered: step t+1 writes the other half.
+      RedEntry* slotr = red + rbuf * NW;
+      rbuf ^= 1;
       const int bad = __any_sync(0xffffffffu, !ok) ? 1 : 0;
       if (lane == 0) {
         slotr[warp].kmax = kmax;
@@ -504,31 +575,30 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
         slotr[warp].abort = bad;
       }
       named_bar_sync(1, NT);
-      int any_bad = 0;
-#pragma unroll 4
-      for (int w = 0; w < NW; ++w) {
-        const Key a1 = static_cast<Key>(slotr[w].kmax), a2 = static_cast<Key>(slotr[w].kmin);
-        kmax = a1 > kmax ? a1 : kmax;
-        kmin = a2 < kmin ? a2 : kmin;
-        any_bad |= slotr[w].abort;
+      Key k1 = T::key(T::lowest()), k2 = T::key(T::highest());
+      int b = 0;
+      if (lane < NW) {
+        k1 = static_cast<Key>(slotr[lane].kmax);
+        k2 = static_cast<Key>(slotr[lane].kmin);
+        b = slotr[lane].abort;
       }
-      if (any_bad) {
+      kmax = T::wmax(k1);
+      kmin = T::wmin(k2);
+      if (__any_sync(0xffffffffu, b)) {
         if (tid == 0) {
-          set_error(a.err, kDevTimeoutFull);
+          set_error(a.err, kDevTimeoutFull, sa, static_cast<int>(parity), static_cast<int>(t));
           *abort_flag = 1;
         }
         return;
       }
-      mx = T::unkey(kmax);
-      mn = T::unkey(kmin);
     } else if (__any_sync(0xffffffffu, !ok)) {
       if (lane == 0) {
-        set_error(a.err, kDevTimeoutFull);
+        set_error(a.err, kDevTimeoutFull, sa, static_cast<int>(parity), static_cast<int>(t));
         *abort_flag = 1;
       }
       return;
     }
-    const Real alpha = T::alpha(mx, mn, u);
+    const Real alpha = T::alpha(T::unkey(kmax), T::unkey(kmin), u);
     const double a64 = static_cast<double>(alpha);
     // x update: entry j belongs to consumer thread j % NT.
     if (kind == kCoord) {
@@ -543,21 +613,24 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
         if (idx % NT == tid) xs[idx] = __fma_rn(a64, T::coef(M.ks_coef[q]), xs[idx]);
       }
     }
-    if (t % a.thinning == 0) {
-      const size_t row = static_cast<size_t>(t / a.thinning) * a.out_nchains + gchain;
+    if (thin_ctr == 0) {
       if (a.out_f64) {
-        double* out = reinterpret_cast<double*>(a.samples) + row * d;
+        double* out = reinterpret_cast<double*>(a.samples) + out_row * d;
         for (int j = tid; j < d; j += NT) out[j] = xs[j];
       } else {
-        float* out = reinterpret_cast<float*>(a.samples) + row * d;
+        float* out = reinterpret_cast<float*>(a.samples) + out_row * d;
         for (int j = tid; j < d; j += NT) out[j] = __double2float_rn(xs[j]);
       }
+      out_row += static_cast<size_t>(a.out_nchains);
     }
+    if (++thin_ctr == a.thinning) thin_ctr = 0;
+    for_kind([&](auto ae_at) {
 #pragma unroll
-    for (int k = 0; k < R; ++k) {
-      const int r = tid + k * NT;
-      if (r < m) sl[k] = T::slack_update(sl[k], alpha, ae_of(r));
-    }
+      for (int k = 0; k < R; ++k) {
+        const int r = tid + k * NT;
+        if (r < m) sl[k] = T::slack_update(sl[k], alpha, ae_at(r));
+      }
+    });
     __syncwarp();
     if (lane == 0) {
       mbar_arrive(&empty[sa]);
@@ -566,6 +639,10 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
   }
   if (a.X_final) {
     for (int j = tid; j < d; j += NT) a.X_final[static_cast<size_t>(chain_local) * a.ldx + j] = xs[j];
+  }
+  if (a.wait_cycles && tid == 0) {
+    a.wait_cycles[4 * chain_local + 0] = w_full;
+    a.wait_cycles[4 * chain_local + 2] = clock64() - c_start;
   }
 }
 

@@ -18,8 +18,13 @@ enum DeviceError : int {
   kDevBadPair = 4,       // a pair schedule index outside [0, d)
 };
 
-__device__ __forceinline__ void set_error(int* err, int code) {
-  if (err) atomicCAS(err, 0, code);
+// The error word is err[0]; err[1..3] hold detail of the first error.
+__device__ __forceinline__ void set_error(int* err, int code, int i0 = 0, int i1 = 0, int i2 = 0) {
+  if (err && atomicCAS(err, 0, code) == 0) {
+    err[1] = i0;
+    err[2] = i1;
+    err[3] = i2;
+  }
 }
 
 __device__ __forceinline__ uint64_t global_ns() {

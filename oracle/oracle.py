@@ -126,3 +126,65 @@ def split_rhat(samples, n_chains, layout=1):
 def ess_series(x):
     x = np.ascontiguousarray(np.asarray(x, dtype=np.float64))
     return load().oracle_ess_series(_p(x), len(x))
+
+
+# ---------------------------------------------------------------- reference
+REF_LIB = HERE / "_ref" / "libnaja_ref.so"
+_ref = None
+
+
+def reference_available() -> bool:
+    return REF_LIB.exists()
+
+
+def _load_ref():
+    global _ref
+    if _ref is None:
+        lib = C.CDLL(str(REF_LIB))
+        vp, i, d = C.c_void_p, C.c_int, C.c_double
+        lib.ref_chr_run.argtypes = [vp, i, i, vp, vp, i, i, i, i, i, d, i, d, i, i, vp, vp, vp, vp, i,
+                                    vp, i, vp, vp, vp, vp]
+        lib.ref_chr_run.restype = i
+        lib.ref_last_error.restype = C.c_char_p
+        _ref = lib
+    return _ref
+
+
+def reference_chr_run(A, b, X0, nspc, thinning, nchains, *, tpb=128, seed=0, pair_prob=0.0, resync_interval=0,
+                      ksparse_prob=0.0, ksparse_k=8, pair_mode=1, pairs=None, T=None, shift=None,
+                      want_samples=True):
+    """The reference's own CoordinateHitAndRun[+backmap_into] (oracle/_ref build).
+
+    Returns (samples (nspc*nchains, d) or None, V (nspc*nchains, n) or None, sampling_ms)."""
+    A = np.asfortranarray(np.asarray(A, dtype=np.float64))
+    m, d = A.shape
+    b = np.ascontiguousarray(np.asarray(b, dtype=np.float64).reshape(-1))
+    X = np.asarray(X0, dtype=np.float64)
+    if X.ndim == 1:
+        X = np.broadcast_to(X, (nchains, d))
+    X = np.ascontiguousarray(X)  # (nchains, d) row-major == d x nchains column-major
+    N = nspc * nchains
+    S = np.empty((N, d), dtype=np.float64) if want_samples else None
+    V = Tm = sh = None
+    n = 0
+    if T is not None:
+        Tm = np.asfortranarray(np.asarray(T, dtype=np.float64))
+        n = Tm.shape[0]
+        sh = np.ascontiguousarray(np.asarray(shift, dtype=np.float64))
+        V = np.empty((N, n), dtype=np.float64) if want_samples else None
+    pi = pj = pc = ps = None
+    npairs = 0
+    if pairs is not None:
+        pi = np.ascontiguousarray(np.asarray(pairs[0], dtype=np.int32))
+        pj = np.ascontiguousarray(np.asarray(pairs[1], dtype=np.int32))
+        pc = np.ascontiguousarray(np.asarray(pairs[2], dtype=np.float64))
+        ps = np.ascontiguousarray(np.asarray(pairs[3], dtype=np.float64))
+        npairs = len(pi)
+    ms = C.c_double(0.0)
+    lib = _load_ref()
+    st = lib.ref_chr_run(_p(A), m, d, _p(b), _p(X), int(nspc), int(thinning), int(nchains), int(tpb), int(seed),
+                         float(pair_prob), int(resync_interval), float(ksparse_prob), int(ksparse_k), int(pair_mode),
+                         _p(pi), _p(pj), _p(pc), _p(ps), npairs, _p(Tm), n, _p(sh), _p(S), _p(V), C.byref(ms))
+    if st != 0:
+        raise RuntimeError("reference run failed: " + lib.ref_last_error().decode())
+    return S, V, ms.value
