@@ -137,8 +137,13 @@ class Workload:
                 "l2": "256 MiB buffer written between timed steps"}
 
 
-def _gate(torch, W, samples_dev, ess, rhat, V_dev):
-    """split-R-hat and bounds checks on the fp32 output (outside the timed region)."""
+def _gate(torch, W, samples_dev, ess, rhat):
+    """split-R-hat and bounds checks on the fp32 output (outside the timed region).
+
+    Polytope rows: A y <= b + 1e-6 max(1, |b|) on every sample.  GEM bounds:
+    the reference's rule (src/validate/bounds_check.cpp:8-39): v = T y + shift
+    in FP64 from the fp32 samples, violation when max(l - v, v - u) - 1e-6 > 0,
+    on <= 1000 evenly spaced samples."""
     A = torch.from_numpy(W.A).to(samples_dev.device)
     b = torch.from_numpy(W.b).to(samples_dev.device)
     tol = 1e-6 * torch.clamp(b.abs(), min=1.0)
@@ -148,15 +153,48 @@ def _gate(torch, W, samples_dev, ess, rhat, V_dev):
         r = samples_dev[s0:s0 + 20000].double() @ A.T - b
         viol += int((r > tol).sum())
         worst = max(worst, float(r.max()))
-    # GEM bounds on <= 1000 back-transformed samples (bounds_check.cpp:8-39 rule, eps 1e-6)
-    step = max(1, V_dev.shape[0] // 1000)
-    v = V_dev[::step].double()
+    step = max(1, samples_dev.shape[0] // 1000)
+    y = samples_dev[::step].double()
+    T = torch.from_numpy(W.T).to(y.device)
+    v = y @ T.T + torch.from_numpy(W.shift).to(y.device)
     u = torch.from_numpy(W.g["u"]).to(v.device)
     lo = torch.from_numpy(W.g["l"]).to(v.device)
     gem = torch.maximum(lo - v - 1e-6, v - u - 1e-6)
     return {"rhat_max": float(np.max(rhat)), "rhat_gate_1_01": bool(np.max(rhat) < 1.01),
             "bounds_violations": viol, "bounds_worst": worst,
             "gem_bounds_violations": int((gem > 0).sum()), "gem_bounds_checked": int(gem.numel())}
+
+
+def _backmap_error(torch, W, samples_dev, V_dev, mode):
+    """Backmap error of `mode` against an FP64 GEMM on 4096 evenly spaced samples."""
+    step = max(1, samples_dev.shape[0] // 4096)
+    y = samples_dev[::step].double()
+    T = torch.from_numpy(W.T).to(y.device)
+    sh = torch.from_numpy(W.shift).to(y.device)
+    ref = y @ T.T + sh
+    got = V_dev[::step].double()
+    scale = y.abs() @ T.abs().T + sh.abs()
+    err = (got - ref).abs()
+    nz = ref.abs() > 1e-3 * ref.abs().max()
+    rel = err[nz] / ref.abs()[nz]
+    return {"mode": mode, "samples": int(y.shape[0]), "max_rel": float(rel.max()),
+            "rms_rel": float(torch.sqrt((rel ** 2).mean())),
+            "max_normalised": float((err / scale.clamp(min=1e-300)).max()),
+            "note": "relative error over |v| > 1e-3 max|v|; normalised = |err| / (|T||y| + |shift|)"}
+
+
+def _backmap_roofline(W, ms, mode):
+    flops = 2.0 * W.n * W.d * W.nspc * W.nchains
+    p = ROOT / "MEASURED_PEAKS.json"
+    bf16 = float(json.loads(p.read_text())["bf16_tflops"]) if p.exists() else 1590.0
+    src = "measured" if p.exists() else "fallback"
+    if mode == "fp64":
+        return {"bound": "fp64 SIMT", "achieved": flops / (ms / 1e3) / 1e12, "unit": "TFLOP/s", "flops": flops}
+    peak = bf16 if mode == "bf16x3" else bf16 / 2.0
+    ach = flops / (ms / 1e3) / 1e12
+    return {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "flops": flops,
+            "peak_source": f"{src} bf16" + ("" if mode == "bf16x3" else " / 2 (tf32 rate)"),
+            "note": "algorithmic FLOPs 2 n d N; the three split products are not credited"}
 
 
 def _cpu_baseline(W, a, min_ess_per_step):
@@ -237,6 +275,7 @@ def _ours(a, rank, world):
         total_ms = float(t.item())
     job_ms = [ev[k][0].elapsed_time(ev[k][1]) for k in range(a.steps)]
     chr_ms = [ev[k][0].elapsed_time(mids[k]) for k in range(a.steps)]
+    bm_ms = [mids[k].elapsed_time(ev[k][1]) for k in range(a.steps)]
     # metric on the last job's samples
     ess, rhat = nv.ess_rhat(samples, W.nchains, layout=1)
     per_dim = ess.sum(axis=1)
@@ -247,7 +286,8 @@ def _ours(a, rank, world):
     min_ess = float(per_dim.min())
     ms_per_step = total_ms / a.steps
     value = min_ess / (ms_per_step / 1e3)  # min-ESS already sums every rank's chains
-    gate = _gate(torch, W, samples, ess, rhat, V)
+    gate = _gate(torch, W, samples, ess, rhat)
+    bm_err = _backmap_error(torch, W, samples, V, a.backmap_mode)
     ref_sem = nv.summary(*nv.ess_rhat(samples, W.nchains, layout=0))
     peak, peak_kind = _peaks()
     chr_mean = statistics.mean(chr_ms)
@@ -263,8 +303,11 @@ def _ours(a, rank, world):
                      "kernel_ms": chr_mean, "bytes_per_chr_step": W.bytes_per_step, "chr_steps_per_launch": W.steps},
         "chr_steps_per_s": steps_per_s, "min_ess": min_ess, "job_ms": job_ms, "chr_ms": chr_ms,
         "gate": gate,
+        "backmap": {"mode": a.backmap_mode, "ms": statistics.mean(bm_ms), "error_vs_fp64": bm_err,
+                    "roofline": _backmap_roofline(W, statistics.mean(bm_ms), a.backmap_mode)},
         "reference_semantics_validate": {k: ref_sem[k] for k in ("status", "ess", "rhat")},
-        "gpu_launches": 2 * a.steps,
+        # per step: the CHR kernel, then the backmap (one FP64 kernel, or operand split x2 + tcgen05 GEMM)
+        "gpu_launches": a.steps * (1 + (1 if a.backmap_mode == "fp64" else 3)),
     }
     line["clocks"] = clk.summary()
     if a.e2e and rank == 0:
@@ -305,40 +348,82 @@ def _e2e(a, W, torch, dev, min_ess):
 def _reference_arm(a, rank, world):
     """The reference's own implementation of the path, timed on this box.
 
-    The reference implements CHR only as CUDA (src/gpu/chr.cu); it has no
-    CPU sampler.  When its sources were compiled here (oracle/_ref/) this arm
-    runs them through their own API; otherwise it times the CPU restatement
-    of the same algorithm (oracle/) with all host threads.
+    The reference implements CHR only in CUDA (src/gpu/chr.cu of
+    quothbonney/naja); it has no CPU sampler.  Its sources, compiled
+    unmodified for sm_100a into oracle/_ref/, are run through their own API
+    (CoordinateHitAndRun, then backmap_into as CoordinateHitAndRunBackmap
+    does) with the reference's defaults: FP64, cuRAND MRG32k3a, 128 threads
+    per chain.  Time = the call plus cudaDeviceSynchronize, as
+    src/engine/job_sampling.cu measures sampling.  Each step is a bounded
+    sample of the workload (fewer samples per chain, same chains, polytope,
+    thinning and pair-prob); its min-ESS comes from the CPU oracle's ESS on
+    the reference's own samples.  Without the reference build the CPU
+    restatement of the same algorithm (oracle/) is timed instead.
     """
     import oracle.oracle as O
 
     W = Workload(a)
-    cores = os.cpu_count() or 1
-    nspc = 2
-    t0 = time.perf_counter()
-    O.chr_run(W.A, W.b, W.start, nspc, W.thin, W.nchains, seed=a.seed, pair_prob=W.pair, precision="fp64",
-              threads=min(cores, W.nchains))
-    dt = time.perf_counter() - t0
-    nspc = max(2, min(W.nspc, int(nspc * a.cpu_seconds / max(dt, 1e-3))))
-    times = []
-    for k in range(a.warmup + a.steps):
+    if O.reference_available() and not a.ref_cpu:
+        cal_nspc = 20
+        # two calibration runs separate the per-call setup from the per-sample time
+        _, _, ms_a = O.reference_chr_run(W.A, W.b, W.start, cal_nspc, W.thin, W.nchains, tpb=128, seed=a.seed,
+                                         pair_prob=W.pair, T=W.T, shift=W.shift, want_samples=False)
+        _, _, ms_b = O.reference_chr_run(W.A, W.b, W.start, 10 * cal_nspc, W.thin, W.nchains, tpb=128,
+                                         seed=a.seed, pair_prob=W.pair, T=W.T, shift=W.shift, want_samples=False)
+        per_sample_ms = max(1e-6, (ms_b - ms_a) / (9 * cal_nspc))
+        # The full workload per timed step unless K steps would exceed the time
+        # budget; warm-up steps are short runs (they only warm the context,
+        # module loading and cuBLAS).
+        nspc = int(max(50, min(W.nspc, a.ref_budget_s * 1e3 / (a.steps * per_sample_ms))))
+        times = []
+        S = None
+        for k in range(a.warmup + a.steps):
+            timed = k >= a.warmup
+            last = k == a.warmup + a.steps - 1
+            S_k, _, ms = O.reference_chr_run(W.A, W.b, W.start, nspc if timed else cal_nspc, W.thin, W.nchains,
+                                             tpb=128, seed=a.seed, pair_prob=W.pair, T=W.T, shift=W.shift,
+                                             want_samples=last, want_v=False)
+            if timed:
+                times.append(ms / 1e3)
+            if last:
+                S = S_k
+        kind, cores = "reference", 0
+        sample = (f"reference CoordinateHitAndRun + backmap_into (FP64, cuRAND MRG32k3a, 128 threads/chain) "
+                  f"compiled from its sources for sm_100a: {W.nchains} chains x {nspc} samples (thinning {W.thin}) "
+                  f"of the {W.nspc}-sample workload per timed step; warm-up steps {cal_nspc} samples; min-ESS "
+                  f"from its own samples")
+        dtype = "f64"
+    else:
+        cores = os.cpu_count() or 1
+        nspc = 2
         t0 = time.perf_counter()
-        S = O.chr_run(W.A, W.b, W.start, nspc, W.thin, W.nchains, seed=a.seed, pair_prob=W.pair, precision="fp64",
-                      threads=min(cores, W.nchains))
-        if k >= a.warmup:
-            times.append(time.perf_counter() - t0)
+        O.chr_run(W.A, W.b, W.start, nspc, W.thin, W.nchains, seed=a.seed, pair_prob=W.pair, precision="fp64",
+                  threads=min(cores, W.nchains))
+        dt = time.perf_counter() - t0
+        nspc = max(50, min(W.nspc, int(nspc * a.cpu_seconds / max(dt, 1e-3))))
+        times = []
+        for k in range(a.warmup + a.steps):
+            t0 = time.perf_counter()
+            S = O.chr_run(W.A, W.b, W.start, nspc, W.thin, W.nchains, seed=a.seed, pair_prob=W.pair,
+                          precision="fp64", threads=min(cores, W.nchains))
+            if k >= a.warmup:
+                times.append(time.perf_counter() - t0)
+        kind, cores = "port", min(cores, W.nchains)
+        sample = (f"CPU restatement of the reference kernel (FP64), {cores} threads: {W.nchains} chains x {nspc} "
+                  f"samples (thinning {W.thin}), no backmap")
+        dtype = "f64"
     dt = statistics.mean(times)
     steps_s = W.nchains * nspc * W.thin / dt
-    # min-ESS per CHR step from the sample itself (chain-correct, summed over chains)
-    ess = O.ess(S.astype(np.float32), W.nchains, layout=1).sum(axis=1).min()
-    value = float(ess) / dt
+    ess = O.ess_fft(S.astype(np.float32), W.nchains, layout=1).sum(axis=1)
+    rhat = O.split_rhat(S.astype(np.float32), W.nchains, layout=1)
+    min_ess = float(ess.min())
+    value = min_ess / dt
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded genome-shaped generator)",
-            "config": W.config(a), "chr_steps_per_s": steps_s,
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": min(cores, W.nchains), "kind": "port",
-                             "sample": f"{W.nchains} chains x {nspc} samples (thinning {W.thin}), FP64 CPU "
-                                       f"restatement of the reference kernel, no backmap"},
+            "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded genome-shaped generator)",
+            "config": W.config(a), "chr_steps_per_s": steps_s, "min_ess": min_ess, "rhat_max": float(rhat.max()),
+            "samples_per_chain_timed": nspc,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     return line
 
@@ -356,17 +441,25 @@ def main(argv=None):
     ap.add_argument("--thinning", type=int, default=116)
     ap.add_argument("--pair-prob", type=float, default=0.3)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--resync", type=int, default=0)
-    ap.add_argument("--backmap-mode", default="fp64", choices=["fp64", "bf16x3", "tf32x3"])
+    ap.add_argument("--resync", type=int, default=2048)
+    ap.add_argument("--backmap-mode", default="tf32x3", choices=["fp64", "bf16x3", "tf32x3"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-budget-s", type=float, default=200.0,
+                    help="reference arm: time budget of the K timed steps")
+    ap.add_argument("--ref-cpu", action="store_true", help="reference arm: time the CPU restatement")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     a = ap.parse_args(argv)
     if a.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if a.impl == "reference":
+        # rank 0 alone times the reference; the other ranks exit without work
+        if rank == 0:
+            print(json.dumps(_reference_arm(a, rank, world)))
+        return
     if world > 1:
         import datetime
 
@@ -375,10 +468,7 @@ def main(argv=None):
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     try:
-        if a.impl == "reference":
-            line = _reference_arm(a, rank, world) if rank == 0 else None
-        else:
-            line = _ours(a, rank, world)
+        line = _ours(a, rank, world)
         if rank == 0 and line is not None:
             print(json.dumps(line))
     finally:

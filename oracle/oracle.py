@@ -152,7 +152,7 @@ def _load_ref():
 
 def reference_chr_run(A, b, X0, nspc, thinning, nchains, *, tpb=128, seed=0, pair_prob=0.0, resync_interval=0,
                       ksparse_prob=0.0, ksparse_k=8, pair_mode=1, pairs=None, T=None, shift=None,
-                      want_samples=True):
+                      want_samples=True, want_v=True):
     """The reference's own CoordinateHitAndRun[+backmap_into] (oracle/_ref build).
 
     Returns (samples (nspc*nchains, d) or None, V (nspc*nchains, n) or None, sampling_ms)."""
@@ -171,7 +171,7 @@ def reference_chr_run(A, b, X0, nspc, thinning, nchains, *, tpb=128, seed=0, pai
         Tm = np.asfortranarray(np.asarray(T, dtype=np.float64))
         n = Tm.shape[0]
         sh = np.ascontiguousarray(np.asarray(shift, dtype=np.float64))
-        V = np.empty((N, n), dtype=np.float64) if want_samples else None
+        V = np.empty((N, n), dtype=np.float64) if (want_samples and want_v) else None
     pi = pj = pc = ps = None
     npairs = 0
     if pairs is not None:
@@ -188,3 +188,40 @@ def reference_chr_run(A, b, X0, nspc, thinning, nchains, *, tpb=128, seed=0, pai
     if st != 0:
         raise RuntimeError("reference run failed: " + lib.ref_last_error().decode())
     return S, V, ms.value
+
+
+def ess_fft(samples, n_chains, layout=1):
+    """Geyer ESS per (dim, chain) with an FFT autocovariance (numpy, FP64).
+
+    The same estimator as `ess` (mcmc.cpp:59-76), evaluated for whole
+    batches of series at once; used where the direct-sum oracle would be too
+    slow (long, slowly mixing chains)."""
+    s = np.asarray(samples, dtype=np.float64)
+    N, dim = s.shape
+    spc = N // n_chains
+    if layout == 1:
+        x = s[: spc * n_chains].reshape(spc, n_chains, dim).transpose(2, 1, 0)  # dim, chain, t
+    else:
+        x = s[: spc * n_chains].reshape(n_chains, spc, dim).transpose(2, 0, 1)
+    out = np.empty((dim, n_chains))
+    nfft = 1 << int(np.ceil(np.log2(2 * spc)))
+    for d0 in range(0, dim, 64):
+        blk = x[d0:d0 + 64]
+        y = blk - blk.mean(axis=2, keepdims=True)
+        f = np.fft.rfft(y, nfft, axis=2)
+        acov = np.fft.irfft(f * np.conj(f), nfft, axis=2)[:, :, :spc] / spc
+        var = acov[:, :, 0]
+        rho = acov / np.where(var > 1e-30, var, 1.0)[:, :, None]
+        kmax = spc // 2
+        pairs = rho[:, :, 1:2 * kmax - 1:2][:, :, : kmax - 1] + rho[:, :, 2:2 * kmax:2][:, :, : kmax - 1]
+        neg = pairs < 0
+        first = np.where(neg.any(axis=2), neg.argmax(axis=2), pairs.shape[2])
+        csum = np.concatenate([np.zeros(pairs.shape[:2] + (1,)), np.cumsum(pairs, axis=2)], axis=2)
+        tau = 1.0 + 2.0 * np.take_along_axis(csum, first[:, :, None], axis=2)[:, :, 0]
+        tau = np.maximum(tau, 1.0)
+        e = spc / tau
+        e[var < 1e-30] = 1.0
+        out[d0:d0 + 64] = e
+    if spc < 4:
+        out[:] = spc
+    return out

@@ -149,3 +149,11 @@ def test_split_rhat_known():
     assert np.all(O.split_rhat(shifted, 4, layout=1) > 1.2)
     # the reference's windows see every chain in every window: no signal
     assert np.all(O.split_rhat(shifted, 4, layout=0) < 1.01)
+
+
+def test_fft_ess_matches_direct_oracle():
+    rng = np.random.default_rng(0)
+    S = (np.cumsum(rng.standard_normal((4000, 5)), axis=0) * 0.05 + rng.standard_normal((4000, 5))).astype(np.float32)
+    for layout in (0, 1):
+        a, b = O.ess(S, 4, layout=layout), O.ess_fft(S, 4, layout=layout)
+        assert np.abs(a - b).max() <= 1e-9 * np.abs(a).max()
