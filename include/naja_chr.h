@@ -123,6 +123,23 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* params, const do
 int naja_backmap(int n, int d, long long N, const double* T, int ldt, const double* shift,
                  const void* Y, int y_dtype, void* V, int v_dtype, int mode, void* stream);
 
+/* The same tensor-core backmap (modes NAJA_BACKMAP_BF16X3 / TF32X3 only)
+ * without allocating device memory: for callers that must not allocate at
+ * the point of the call, such as a service that reserves its device-memory
+ * budget up front and forbids allocations on its request path, or a host
+ * framework whose allocator owns the device.  No counterpart in the
+ * reference.  T, shift, Y and V must be device memory.  The split operands
+ * use a 64 MiB array that every device loading the library holds until
+ * process exit; a call needing more (about 1 KiB + 2 * N * dp * e +
+ * 2 * n * dp * e bytes, dp = d rounded up to 64, e = 2 for BF16X3 and 4
+ * for TF32X3) is rejected with NAJA_ERR_INVALID_ARGUMENT: split N across
+ * calls.  The first call on a device looks the array up on that device;
+ * make it before any stream capture.  Calls share the array: calls whose
+ * work overlaps on the GPU race.  Synchronises `stream` to read its error
+ * word. */
+int naja_backmap_noalloc(int n, int d, long long N, const double* T, int ldt, const double* shift,
+                         const void* Y, int y_dtype, void* V, int v_dtype, int mode, void* stream);
+
 /* ------------------------------------------------------------ validate */
 
 /* Geyer ESS per (dim, chain) and split-R-hat per dim of an (N, dim)

@@ -37,6 +37,7 @@ EXPORTED = (
     "naja_polytope_check",
     "naja_chr_run",
     "naja_backmap",
+    "naja_backmap_noalloc",
     "naja_validate",
     "naja_last_error",
     "naja_mrg_state_bytes",
@@ -111,6 +112,7 @@ def load() -> C.CDLL:
     lib.naja_polytope_check.argtypes = [vp]
     lib.naja_chr_run.argtypes = [vp, C.POINTER(ChrParams), vp, i, vp, vp, vp]
     lib.naja_backmap.argtypes = [i, i, ll, vp, i, vp, vp, i, vp, i, i, vp]
+    lib.naja_backmap_noalloc.argtypes = [i, i, ll, vp, i, vp, vp, i, vp, i, i, vp]
     lib.naja_validate.argtypes = [vp, ll, i, i, i, vp, vp, vp]
     lib.naja_last_error.restype = C.c_char_p
     lib.naja_last_error.argtypes = []
@@ -121,7 +123,7 @@ def load() -> C.CDLL:
     for name in EXPORTED:
         f = getattr(lib, name)
         if f.restype is C.c_int or name in ("naja_polytope_create", "naja_polytope_destroy", "naja_polytope_shape",
-                                               "naja_polytope_check", "naja_chr_run", "naja_backmap",
+                                               "naja_polytope_check", "naja_chr_run", "naja_backmap", "naja_backmap_noalloc",
                                                "naja_validate", "naja_mrg_tape", "naja_mrg_init_states"):
             f.restype = C.c_int
     _lib = lib

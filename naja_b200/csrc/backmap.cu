@@ -24,6 +24,8 @@ namespace naja {
 
 int backmap_tc(int n, int d, long long N, const double* T, int ldt, const double* shift, const void* Y, int y_dtype,
                void* V, int v_dtype, int mode, cudaStream_t stream);
+int backmap_tc_noalloc(int n, int d, long long N, const double* T, int ldt, const double* shift, const void* Y,
+                       int y_dtype, void* V, int v_dtype, int mode, cudaStream_t stream);
 
 namespace {
 
@@ -142,4 +144,20 @@ extern "C" int naja_backmap(int n, int d, long long N, const double* T, int ldt,
   if (e == cudaSuccess && (host_v || bT.ptr || bs.ptr || bY.ptr)) e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("backmap: ") + cudaGetErrorString(e));
   return NAJA_OK;
+}
+
+extern "C" int naja_backmap_noalloc(int n, int d, long long N, const double* T, int ldt, const double* shift,
+                                    const void* Y, int y_dtype, void* V, int v_dtype, int mode, void* stream_ptr) {
+  if (n <= 0 || d <= 0 || N < 0) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_backmap_noalloc: bad shape");
+  if (!T || !shift || !Y || !V) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_backmap_noalloc: null argument");
+  if (ldt < n) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_backmap_noalloc: ldt < n");
+  if ((y_dtype != NAJA_DTYPE_F32 && y_dtype != NAJA_DTYPE_F64) || (v_dtype != NAJA_DTYPE_F32 && v_dtype != NAJA_DTYPE_F64))
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_backmap_noalloc: unknown dtype");
+  if (mode != NAJA_BACKMAP_BF16X3 && mode != NAJA_BACKMAP_TF32X3)
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_backmap_noalloc: mode must be NAJA_BACKMAP_BF16X3 or NAJA_BACKMAP_TF32X3");
+  // Host buffers would need staging copies, i.e. allocations: every buffer must be device memory.
+  if (!is_device_ptr(T) || !is_device_ptr(shift) || !is_device_ptr(Y) || !is_device_ptr(V))
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_backmap_noalloc: T, shift, Y and V must be device memory");
+  if (N == 0) return NAJA_OK;
+  return backmap_tc_noalloc(n, d, N, T, ldt, shift, Y, y_dtype, V, v_dtype, mode, static_cast<cudaStream_t>(stream_ptr));
 }

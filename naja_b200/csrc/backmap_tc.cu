@@ -26,6 +26,7 @@
 #include <cudaTypedefs.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 
 #include "../../include/naja_chr.h"
@@ -443,6 +444,121 @@ int backmap_tc(int n, int d, long long N, const double* T, int ldt, const double
     return fail(NAJA_ERR_DEVICE, "backmap: tensor-core pipeline gave up a bounded wait (code " + std::to_string(w[0]) +
                                      ", " + std::to_string(w[1]) + ", " + std::to_string(w[2]) + ", " +
                                      std::to_string(w[3]) + ")");
+  return NAJA_OK;
+}
+
+// ----------------------------------------------------------------------
+// Allocation-free variant (naja_backmap_noalloc).
+//
+// Some callers cannot allocate device memory at the point they need the
+// backmap: a service that reserves its whole device-memory budget up front
+// and forbids allocations in its request path, or a host framework whose
+// allocator owns the device and must not see cudaMalloc/cudaFree (which may
+// also synchronise the device) from a library.  For them the split operands
+// live in one file-scope device array of fixed size instead of per-call
+// buffers.  The array exists once per device that loads this library and is
+// held until the process exits.  Its device address is looked up once per
+// device (cudaGetSymbolAddress, with that device current) on the first call
+// made on that device; that first call should therefore come before any
+// stream capture.  Every call reuses the same array: the error words are
+// cleared by each call, and calls whose work overlaps on the GPU (different
+// streams, or different host threads on one device) race on the array.
+constexpr size_t kNoAllocScratchBytes = 64ull << 20;  // 64 MiB
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+int noalloc_scratch(unsigned char** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_backmap_noalloc: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(NAJA_ERR_UNSUPPORTED, "naja_backmap_noalloc: device index too large");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(NAJA_ERR_CUDA, std::string("naja_backmap_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return NAJA_OK;
+}
+}  // namespace
+
+int backmap_tc_noalloc(int n, int d, long long N, const double* T, int ldt, const double* shift, const void* Y,
+                       int y_dtype, void* V, int v_dtype, int mode, cudaStream_t stream) {
+  const bool tf32 = mode == NAJA_BACKMAP_TF32X3;
+  const int esz = tf32 ? 4 : 2;
+  const int dp = (d + 63) / 64 * 64;
+  // scratch layout: [error words | Y hi | Y lo | T hi | T lo], each 1024-aligned
+  auto up = [](size_t v) { return (v + 1023) / 1024 * 1024; };
+  const size_t ybytes = up(static_cast<size_t>(N) * dp * esz), tbytes = up(static_cast<size_t>(n) * dp * esz);
+  const size_t need = 1024 + 2 * ybytes + 2 * tbytes;
+  if (need > kNoAllocScratchBytes)
+    return fail(NAJA_ERR_INVALID_ARGUMENT,
+                "naja_backmap_noalloc: this shape needs " + std::to_string(need) + " bytes of scratch, more than the " +
+                    std::to_string(kNoAllocScratchBytes) + " the library reserves; pass fewer samples per call");
+  unsigned char* base = nullptr;
+  int st = noalloc_scratch(&base);
+  if (st) return st;
+  int* err = reinterpret_cast<int*>(base);
+  void* Yh = base + 1024;
+  void* Yl = base + 1024 + ybytes;
+  void* Th = base + 1024 + 2 * ybytes;
+  void* Tl = base + 1024 + 2 * ybytes + tbytes;
+  cudaError_t e = cudaMemsetAsync(err, 0, 4 * sizeof(int), stream);
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_backmap_noalloc: ") + cudaGetErrorString(e));
+  const int sblocks = 148 * 8;
+  if (tf32) {
+    if (y_dtype == NAJA_DTYPE_F64)
+      split_rows_kernel<double, true><<<sblocks, 256, 0, stream>>>(static_cast<const double*>(Y), N, d, dp, Yh, Yl);
+    else
+      split_rows_kernel<float, true><<<sblocks, 256, 0, stream>>>(static_cast<const float*>(Y), N, d, dp, Yh, Yl);
+    split_T_kernel<true><<<sblocks, 256, 0, stream>>>(T, ldt, n, d, dp, Th, Tl);
+  } else {
+    if (y_dtype == NAJA_DTYPE_F64)
+      split_rows_kernel<double, false><<<sblocks, 256, 0, stream>>>(static_cast<const double*>(Y), N, d, dp, Yh, Yl);
+    else
+      split_rows_kernel<float, false><<<sblocks, 256, 0, stream>>>(static_cast<const float*>(Y), N, d, dp, Yh, Yl);
+    split_T_kernel<false><<<sblocks, 256, 0, stream>>>(T, ldt, n, d, dp, Th, Tl);
+  }
+  CUtensorMap mAh, mAl, mBh, mBl;
+  if (!make_map(&mAh, Yh, tf32, N, dp, kTileM) || !make_map(&mAl, Yl, tf32, N, dp, kTileM) ||
+      !make_map(&mBh, Th, tf32, n, dp, kTileN) || !make_map(&mBl, Tl, tf32, n, dp, kTileN))
+    return fail(NAJA_ERR_CUDA, "naja_backmap_noalloc: cuTensorMapEncodeTiled failed");
+  TcArgs a;
+  a.n = n;
+  a.kslices = dp * esz / kSliceBytes;
+  a.N = N;
+  a.tiles_n = (n + kTileN - 1) / kTileN;
+  a.tiles = ((N + kTileM - 1) / kTileM) * a.tiles_n;
+  a.shift = shift;
+  a.V = V;
+  a.v_f64 = v_dtype == NAJA_DTYPE_F64;
+  a.err = err;
+  const size_t smem = kStages * kStageBytes + 1024 + 256;
+  int sms = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = static_cast<int>(std::min<long long>(sms, a.tiles));
+  auto kern = tf32 ? backmap_tc_kernel<true> : backmap_tc_kernel<false>;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_backmap_noalloc: ") + cudaGetErrorString(e));
+  kern<<<grid, kThreads, smem, stream>>>(mAh, mAl, mBh, mBl, a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return fail(NAJA_ERR_CUDA, std::string("naja_backmap_noalloc: launch failed: ") + cudaGetErrorString(e));
+  int w[4] = {0, 0, 0, 0};
+  e = cudaMemcpyAsync(w, err, sizeof(w), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_backmap_noalloc: ") + cudaGetErrorString(e));
+  if (w[0] != 0)
+    return fail(NAJA_ERR_DEVICE, "naja_backmap_noalloc: tensor-core pipeline gave up a bounded wait (code " +
+                                     std::to_string(w[0]) + ")");
   return NAJA_OK;
 }
 
