@@ -314,6 +314,8 @@ def _ours(a, rank, world):
         line["e2e"] = _e2e(a, W, torch, dev, min_ess)
     if rank == 0 and world == 1 and not a.no_cpu:
         line["cpu_baseline"] = _cpu_baseline(W, a, min_ess / W.steps)
+    if rank == 0 and a.batch_models > 0:
+        line["batched"] = _batched(a, torch, dev)
     P.close()
     return line
 
@@ -343,6 +345,65 @@ def _e2e(a, W, torch, dev, min_ess):
     ms = statistics.mean(times)
     return {"value": min_ess / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
             "ms_per_step": ms}
+
+
+def _batched(a, torch, dev):
+    """Conditioned-variant batch: 64 models = the genome-shaped polytope plus
+    0-200 extra rows each (bounds of up to 100 reactions tightened by a factor
+    in [0.05, 0.5], the extra-row rule of cmd_prepare.cpp:111-156), 8 chains x
+    4000 samples per model, thinning 116, pair-prob 0.3 (the genome workload's
+    settings), all in one persistent launch replayed from a CUDA graph; launch
+    shape from the autotuner.  Separate polytopes per model: A is read from
+    HBM (the batch's FP32 A is ~1 GB, far beyond L2)."""
+    import naja_b200 as nb
+    from naja_b200 import autotune, synth
+    from naja_b200.batch import Batch
+
+    base = synth.genome_shaped(n=a.n, d=a.d, density=0.08, seed_T=0, seed_u=1)
+    variants = synth.conditioned_variants(base, a.batch_models, max_reactions=100, seed=2)
+    polys = [nb.Polytope(np.vstack([base["A"], v["extra_A"]]), np.concatenate([base["b"], v["extra_b"]]),
+                         device=dev.index) for v in variants]
+    B = Batch(polys)
+    nch, nspc, thin = a.batch_chains, a.batch_nspc, a.thinning
+    X = [torch.zeros((nch, a.d), dtype=torch.float64, device=dev) for _ in polys]
+    outs = [torch.empty((nspc * nch, a.d), dtype=torch.float32, device=dev) for _ in polys]
+    kw = dict(seed=a.seed, pair_prob=a.pair_prob, resync_interval=a.resync)
+    if a.batch_shape:
+        t_, s_, ss_, c_ = (int(v) for v in a.batch_shape.split(","))
+        from naja_b200.batch import Shape
+
+        shape, table = Shape(t_, s_, ss_, c_), {}
+    else:
+        shape, table = autotune.tune(B, X, outs, nch, thin, **kw)
+    g = B.capture(X, outs, nspc, thin, nch, shape=shape, **kw)
+    g.launch()
+    torch.cuda.synchronize()
+    g.check()
+    times = []
+    for _ in range(max(1, a.steps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.launch()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    g.check()
+    ms = statistics.mean(times)
+    ms_rows = [p.m for p in polys]
+    steps = len(polys) * nch * nspc * thin
+    bytes_total = sum(nch * nspc * thin * (4.0 * m * (1 + a.pair_prob) + 4.0 * a.d / thin) for m in ms_rows)
+    peak, src = _peaks()
+    ach = bytes_total / (ms / 1e3) / 1e9
+    g.close()
+    return {"workload": f"{len(polys)} conditioned variants (m {min(ms_rows)}-{max(ms_rows)}) x {nch} chains x "
+                        f"{nspc} samples, thinning {thin}, pair-prob {a.pair_prob}, one persistent launch in a CUDA graph",
+            "shape": {"threads": shape.threads, "slots": shape.slots, "slack_smem": shape.slack_smem,
+                      "ctas_per_sm": shape.ctas_per_sm},
+            "ms": ms, "chr_steps_per_s": steps / (ms / 1e3),
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                         "peak_source": src, "bytes_per_chr_step": bytes_total / steps},
+            "autotune_top": sorted(({"shape": str(k), "M_steps_per_s": v / 1e6} for k, v in table.items()),
+                                   key=lambda r: -r["M_steps_per_s"])[:5]}
 
 
 def _reference_arm(a, rank, world):
@@ -446,6 +507,10 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--batch-models", type=int, default=64, help="batched-variant section (0 = skip)")
+    ap.add_argument("--batch-chains", type=int, default=8)
+    ap.add_argument("--batch-nspc", type=int, default=4000)
+    ap.add_argument("--batch-shape", default="", help="threads,slots,slack_smem,ctas_per_sm (skips the autotuner)")
     ap.add_argument("--ref-budget-s", type=float, default=200.0,
                     help="reference arm: time budget of the K timed steps")
     ap.add_argument("--ref-cpu", action="store_true", help="reference arm: time the CPU restatement")

@@ -114,6 +114,42 @@ int naja_polytope_check(const naja_polytope* P);
 int naja_chr_run(const naja_polytope* P, const naja_chr_params* params, const double* X0, int ldx,
                  void* samples, double* X_final, void* stream);
 
+/* ------------------------------------------------------------- batches */
+
+/* Launch shape of a batched run (chosen by the autotuner in
+ * naja_b200/autotune.py, or by hand). */
+typedef struct naja_batch_config {
+    int threads;      /* consumer threads per chain: 128, 256 or 512            */
+    int slots;        /* staged-column ring depth 2..8, 0 = direct column reads */
+    int slack_smem;   /* 1: slack in shared memory (several chains per SM)      */
+    int ctas_per_sm;  /* resident chains per SM, 0 = as many as fit             */
+} naja_batch_config;
+
+/* Runs params->nchains chains of each of `nmodels` polytopes (the same d)
+ * in ONE persistent launch.  Model k uses seed params->seed + k*seed_stride
+ * and its chains are numbered 0..nchains-1, so it draws exactly the streams a
+ * standalone naja_chr_run of that model with that seed draws.  X0s[k]
+ * (d x nchains, leading dimension ldx) and samples[k] ((nspc*nchains) x d,
+ * params->out_dtype) are device pointers.  FP32 tier.  This replaces the
+ * reference's model-by-model bulk loop (src/engine/job_bulk.cpp:115-189),
+ * which launches one small CoordinateHitAndRun per model. */
+int naja_chr_run_batched(int nmodels, const naja_polytope* const* models, const naja_chr_params* params,
+                         const double* const* X0s, int ldx, void* const* samples, unsigned long long seed_stride,
+                         const naja_batch_config* config, void* stream);
+/* Resident chains per SM that `config` allows for these models (0 if none). */
+int naja_batch_occupancy(int nmodels, const naja_polytope* const* models, const naja_batch_config* config,
+                         int* ctas_per_sm);
+/* The same batched launch captured once into a CUDA graph (*graph receives
+ * an opaque handle that keeps the launch's descriptors alive); replay it
+ * with naja_graph_launch, check it with naja_graph_check, release it with
+ * naja_graph_destroy. */
+int naja_chr_capture_batched(int nmodels, const naja_polytope* const* models, const naja_chr_params* params,
+                             const double* const* X0s, int ldx, void* const* samples,
+                             unsigned long long seed_stride, const naja_batch_config* config, void** graph);
+int naja_graph_launch(void* graph, void* stream);
+int naja_graph_check(void* graph);
+int naja_graph_destroy(void* graph);
+
 /* ------------------------------------------------------------- backmap */
 
 /* V = T * Y + shift * 1^T.  T is n x d column-major (leading dimension ldt),

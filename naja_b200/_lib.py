@@ -44,6 +44,12 @@ EXPORTED = (
     "naja_mrg_tape",
     "naja_mrg_init_states",
     "naja_version",
+    "naja_chr_run_batched",
+    "naja_batch_occupancy",
+    "naja_chr_capture_batched",
+    "naja_graph_launch",
+    "naja_graph_check",
+    "naja_graph_destroy",
 )
 
 
@@ -76,6 +82,12 @@ class ChrParams(C.Structure):
         ("rng_state", C.c_void_p),
         ("wait_cycles", C.c_void_p),
     ]
+
+
+class BatchConfig(C.Structure):
+    """Mirror of `naja_batch_config`."""
+
+    _fields_ = [("threads", C.c_int), ("slots", C.c_int), ("slack_smem", C.c_int), ("ctas_per_sm", C.c_int)]
 
 
 class NajaError(RuntimeError):
@@ -120,11 +132,22 @@ def load() -> C.CDLL:
     lib.naja_mrg_tape.argtypes = [i, ull, i, i, ll, vp]
     lib.naja_mrg_init_states.argtypes = [i, ull, i, i, vp]
     lib.naja_version.restype = C.c_char_p
+    pp = C.POINTER(C.c_void_p)
+    lib.naja_chr_run_batched.argtypes = [i, pp, C.POINTER(ChrParams), pp, i, pp, ull, C.POINTER(BatchConfig), vp]
+    lib.naja_batch_occupancy.argtypes = [i, pp, C.POINTER(BatchConfig), C.POINTER(i)]
+    lib.naja_chr_capture_batched.argtypes = [i, pp, C.POINTER(ChrParams), pp, i, pp, ull, C.POINTER(BatchConfig),
+                                             C.POINTER(vp)]
+    lib.naja_graph_launch.argtypes = [vp, vp]
+    lib.naja_graph_check.argtypes = [vp]
+    lib.naja_graph_destroy.argtypes = [vp]
     for name in EXPORTED:
         f = getattr(lib, name)
         if f.restype is C.c_int or name in ("naja_polytope_create", "naja_polytope_destroy", "naja_polytope_shape",
                                                "naja_polytope_check", "naja_chr_run", "naja_backmap", "naja_backmap_noalloc",
-                                               "naja_validate", "naja_mrg_tape", "naja_mrg_init_states"):
+                                               "naja_validate", "naja_mrg_tape", "naja_mrg_init_states",
+                                               "naja_chr_run_batched", "naja_batch_occupancy",
+                                               "naja_chr_capture_batched", "naja_graph_launch", "naja_graph_check",
+                                               "naja_graph_destroy"):
             f.restype = C.c_int
     _lib = lib
     return lib

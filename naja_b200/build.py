@@ -36,6 +36,8 @@ def _units():
         for nt in CHR_THREADS:
             units.append((f"chr_{real}_{nt}", CSRC / "chr_inst.cu",
                           ["-fmad=false", f"-DNAJA_CHR_REAL={real}", f"-DNAJA_CHR_NT={nt}"]))
+    for nt in (128, 256, 512):
+        units.append((f"chr_batched_{nt}", CSRC / "chr_batched_inst.cu", ["-fmad=false", f"-DNAJA_CHR_NT={nt}"]))
     units.append(("chr_host", CSRC / "chr_host.cu", ["-fmad=false"]))
     units.append(("capi", CSRC / "capi.cu", []))
     units.append(("validate", CSRC / "validate.cu", ["-fmad=false"]))

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/naja_chr.h"
 #include "capi_internal.cuh"
@@ -382,3 +383,248 @@ int naja_mrg_tape(int device, unsigned long long seed, int chain_base, int nchai
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ batches
+namespace {
+
+struct BatchPrep {
+  ChrArgs base;
+  BatchConfig cfg;
+  std::vector<ModelDesc> descs;
+  std::vector<int> item_model, item_chain;
+  int device = 0;
+};
+
+int prep_batch(int nmodels, const naja_polytope* const* models, const naja_chr_params* p, const double* const* X0s,
+               int ldx, void* const* samples, unsigned long long seed_stride, const naja_batch_config* c,
+               BatchPrep* out) {
+  if (nmodels <= 0 || !models || !p || !X0s || !samples || !c)
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: null or empty argument");
+  if (p->nchains <= 0 || p->nspc <= 0 || p->thinning <= 0)
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: nchains, nspc and thinning must be positive");
+  if (p->precision != NAJA_PREC_FP32)
+    return fail(NAJA_ERR_UNSUPPORTED, "naja_chr_run_batched: the batched kernel runs the FP32 tier");
+  if (p->rng != NAJA_RNG_PHILOX && p->rng != NAJA_RNG_REF_MRG)
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: unknown rng");
+  if (p->rng_state) return fail(NAJA_ERR_UNSUPPORTED, "naja_chr_run_batched: carried MRG states are not supported");
+  if (p->out_dtype != NAJA_DTYPE_F32 && p->out_dtype != NAJA_DTYPE_F64)
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: unknown output dtype");
+  if (p->n_pairs > 0 && (!is_device_ptr(p->pair_i) || !is_device_ptr(p->pair_j) || !is_device_ptr(p->pair_c) ||
+                         !is_device_ptr(p->pair_s)))
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: the pair schedule must be device memory");
+  const int d = models[0] ? models[0]->d : 0;
+  int lda_max = 0, m_max = 0;
+  for (int k = 0; k < nmodels; ++k) {
+    const naja_polytope* P = models[k];
+    if (!P) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: null model");
+    if (P->d != d) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: models differ in d");
+    if (P->device != models[0]->device) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: models on different devices");
+    if (!X0s[k] || !samples[k] || !is_device_ptr(X0s[k]) || !is_device_ptr(samples[k]))
+      return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: X0s and samples must be device pointers");
+    lda_max = std::max(lda_max, P->lda);
+    m_max = std::max(m_max, P->m);
+  }
+  if (ldx < d) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: ldx < d");
+  BatchConfig cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.threads = c->threads;
+  cfg.slots = c->slots;
+  cfg.slack_smem = c->slack_smem;
+  cfg.ctas_per_sm = c->ctas_per_sm;
+  int st = chr_batch_plan(m_max, d, lda_max, &cfg);
+  if (st == NAJA_ERR_INVALID_ARGUMENT) return fail(st, "naja_chr_run_batched: bad batch configuration");
+  if (st) return fail(st, "naja_chr_run_batched: configuration cannot hold models of " + std::to_string(m_max) + " rows");
+  ChrArgs& a = out->base;
+  std::memset(&a, 0, sizeof(a));
+  a.d = d;
+  a.lda = lda_max;
+  a.out_f64 = p->out_dtype == NAJA_DTYPE_F64;
+  a.out_nchains = p->nchains;
+  a.nspc = p->nspc;
+  a.thinning = p->thinning;
+  a.step_offset = p->step_offset;
+  a.pair_prob = p->pair_prob;
+  a.ksparse_prob = p->ksparse_prob;
+  a.ksparse_k = p->ksparse_k;
+  a.pair_mode = p->pair_mode;
+  a.pair_i = p->pair_i;
+  a.pair_j = p->pair_j;
+  a.pair_c = p->pair_c;
+  a.pair_s = p->pair_s;
+  a.n_pairs = p->n_pairs;
+  a.resync = p->resync_interval;
+  a.rng = p->rng;
+  a.err = models[0]->err;
+  a.timeout_ns = kWaitTimeoutNs;
+  out->cfg = cfg;
+  out->device = models[0]->device;
+  out->descs.resize(nmodels);
+  for (int k = 0; k < nmodels; ++k) {
+    const naja_polytope* P = models[k];
+    ModelDesc& m = out->descs[k];
+    m.A32 = P->A32;
+    m.A64 = P->A64;
+    m.lda = P->lda;
+    m.m = P->m;
+    m.b = P->b;
+    m.X0 = X0s[k];
+    m.ldx = ldx;
+    m.samples = samples[k];
+    m.X_final = nullptr;
+    m.seed = p->seed + static_cast<unsigned long long>(k) * seed_stride;
+  }
+  // chains of different models interleave, so resident CTAs spread over models
+  for (int ch = 0; ch < p->nchains; ++ch)
+    for (int k = 0; k < nmodels; ++k) {
+      out->item_model.push_back(k);
+      out->item_chain.push_back(ch);
+    }
+  return NAJA_OK;
+}
+
+size_t batch_bytes(const BatchPrep& b) {
+  return b.descs.size() * sizeof(ModelDesc) + 2 * b.item_model.size() * sizeof(int) + 64;
+}
+
+void batch_pack(const BatchPrep& b, std::vector<unsigned char>& host, void* dev, const ModelDesc** dm, const int** im,
+                const int** ic) {
+  host.assign(batch_bytes(b), 0);
+  size_t off = 0;
+  std::memcpy(host.data(), b.descs.data(), b.descs.size() * sizeof(ModelDesc));
+  *dm = reinterpret_cast<const ModelDesc*>(static_cast<char*>(dev) + off);
+  off += (b.descs.size() * sizeof(ModelDesc) + 15) / 16 * 16;
+  std::memcpy(host.data() + off, b.item_model.data(), b.item_model.size() * sizeof(int));
+  *im = reinterpret_cast<const int*>(static_cast<char*>(dev) + off);
+  off += b.item_model.size() * sizeof(int);
+  std::memcpy(host.data() + off, b.item_chain.data(), b.item_chain.size() * sizeof(int));
+  *ic = reinterpret_cast<const int*>(static_cast<char*>(dev) + off);
+}
+
+struct GraphHandle {
+  int device = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  void* dev = nullptr;
+  int* err = nullptr;
+};
+
+}  // namespace
+
+extern "C" int naja_chr_run_batched(int nmodels, const naja_polytope* const* models, const naja_chr_params* p,
+                                    const double* const* X0s, int ldx, void* const* samples,
+                                    unsigned long long seed_stride, const naja_batch_config* c, void* stream_ptr) {
+  BatchPrep b;
+  int st = prep_batch(nmodels, models, p, X0s, ldx, samples, seed_stride, c, &b);
+  if (st) return st;
+  DeviceGuard g(b.device);
+  cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+  DeviceBuffer buf;
+  if ((st = buf.alloc(batch_bytes(b), stream))) return st;
+  std::vector<unsigned char> host;
+  const ModelDesc* dm;
+  const int *im, *ic;
+  batch_pack(b, host, buf.ptr, &dm, &im, &ic);
+  cudaError_t e = cudaMemcpyAsync(buf.ptr, host.data(), host.size(), cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_chr_run_batched: ") + cudaGetErrorString(e));
+  st = chr_batch_launch(b.base, dm, im, ic, static_cast<int>(b.item_model.size()), b.cfg, stream);
+  if (st) return fail(st, std::string("naja_chr_run_batched: launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+  // the staging copy above is from pageable memory: it has completed when cudaMemcpyAsync returned
+  return NAJA_OK;
+}
+
+extern "C" int naja_batch_occupancy(int nmodels, const naja_polytope* const* models, const naja_batch_config* c,
+                                    int* ctas_per_sm) {
+  if (!ctas_per_sm || !c || nmodels <= 0 || !models || !models[0])
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_batch_occupancy: bad arguments");
+  int lda_max = 0, m_max = 0;
+  for (int k = 0; k < nmodels; ++k) {
+    lda_max = std::max(lda_max, models[k]->lda);
+    m_max = std::max(m_max, models[k]->m);
+  }
+  BatchConfig cfg;
+  std::memset(&cfg, 0, sizeof(cfg));
+  cfg.threads = c->threads;
+  cfg.slots = c->slots;
+  cfg.slack_smem = c->slack_smem;
+  cfg.ctas_per_sm = c->ctas_per_sm;
+  *ctas_per_sm = 0;
+  if (chr_batch_plan(m_max, models[0]->d, lda_max, &cfg) != NAJA_OK) return NAJA_OK;
+  DeviceGuard g(models[0]->device);
+  int st = chr_batch_occupancy(cfg, ctas_per_sm);
+  if (st) *ctas_per_sm = 0;
+  return NAJA_OK;
+}
+
+extern "C" int naja_chr_capture_batched(int nmodels, const naja_polytope* const* models, const naja_chr_params* p,
+                                        const double* const* X0s, int ldx, void* const* samples,
+                                        unsigned long long seed_stride, const naja_batch_config* c, void** graph) {
+  if (!graph) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_capture_batched: graph is null");
+  *graph = nullptr;
+  BatchPrep b;
+  int st = prep_batch(nmodels, models, p, X0s, ldx, samples, seed_stride, c, &b);
+  if (st) return st;
+  DeviceGuard g(b.device);
+  GraphHandle* h = new GraphHandle();
+  h->device = b.device;
+  cudaError_t e = cudaMalloc(&h->dev, batch_bytes(b));
+  if (e == cudaSuccess) e = cudaMalloc(&h->err, 4 * sizeof(int));
+  if (e != cudaSuccess) {
+    naja_graph_destroy(h);
+    return fail(NAJA_ERR_NO_MEMORY, std::string("naja_chr_capture_batched: ") + cudaGetErrorString(e));
+  }
+  std::vector<unsigned char> host;
+  const ModelDesc* dm;
+  const int *im, *ic;
+  batch_pack(b, host, h->dev, &dm, &im, &ic);
+  e = cudaMemcpy(h->dev, host.data(), host.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemset(h->err, 0, 4 * sizeof(int));
+  b.base.err = h->err;
+  int occ = 0;
+  if (e == cudaSuccess) chr_batch_occupancy(b.cfg, &occ);  // sets the kernel's smem attribute outside the capture
+  cudaStream_t s = nullptr;
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed);
+  if (e == cudaSuccess) {
+    st = chr_batch_launch(b.base, dm, im, ic, static_cast<int>(b.item_model.size()), b.cfg, s);
+    cudaError_t e2 = cudaStreamEndCapture(s, &h->graph);
+    if (st == NAJA_OK) e = e2;
+  }
+  if (e == cudaSuccess && st == NAJA_OK) e = cudaGraphInstantiate(&h->exec, h->graph, 0);
+  if (s) cudaStreamDestroy(s);
+  if (e != cudaSuccess || st != NAJA_OK) {
+    naja_graph_destroy(h);
+    return fail(st ? st : NAJA_ERR_CUDA, std::string("naja_chr_capture_batched: ") + cudaGetErrorString(e));
+  }
+  *graph = h;
+  return NAJA_OK;
+}
+
+extern "C" int naja_graph_launch(void* graph, void* stream) {
+  GraphHandle* h = static_cast<GraphHandle*>(graph);
+  if (!h || !h->exec) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_graph_launch: null graph");
+  DeviceGuard g(h->device);
+  cudaError_t e = cudaGraphLaunch(h->exec, static_cast<cudaStream_t>(stream));
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_graph_launch: ") + cudaGetErrorString(e));
+  return NAJA_OK;
+}
+
+extern "C" int naja_graph_check(void* graph) {
+  GraphHandle* h = static_cast<GraphHandle*>(graph);
+  if (!h) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_graph_check: null graph");
+  DeviceGuard g(h->device);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_graph_check: ") + cudaGetErrorString(e));
+  return read_device_error(h->err);
+}
+
+extern "C" int naja_graph_destroy(void* graph) {
+  GraphHandle* h = static_cast<GraphHandle*>(graph);
+  if (!h) return NAJA_OK;
+  DeviceGuard g(h->device);
+  if (h->exec) cudaGraphExecDestroy(h->exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  cudaFree(h->dev);
+  cudaFree(h->err);
+  delete h;
+  return NAJA_OK;
+}

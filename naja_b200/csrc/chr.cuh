@@ -65,6 +65,43 @@ int chr_launch(int precision, const ChrArgs& args, int nchains, const ChrLaunchC
 // MRG32k3a states, c < nchains, into tape[c * count + i] (device memory).
 int mrg_tape(unsigned long long seed, int chain_base, int nchains, long count, double* tape, cudaStream_t stream);
 
+// ---------------------------------------------------------------- batches
+// One model of a batched run: its polytope (padded column-major A, b), start
+// points and outputs.  Every model of a batch shares d and the step settings
+// of the launch's ChrArgs; chains of a model are numbered 0..nchains-1 and
+// draw the streams a standalone run of that model with `seed` draws.
+struct ModelDesc {
+  const float* A32;
+  const double* A64;
+  int lda;
+  int m;
+  const double* b;
+  const double* X0;  // d x nchains, leading dimension ldx
+  int ldx;
+  void* samples;     // (nspc * nchains) x d
+  double* X_final;   // nullable
+  unsigned long long seed;
+};
+
+struct BatchConfig {
+  int threads;      // consumer threads per chain
+  int rows;         // rows per consumer thread (template capacity)
+  int slots;        // ring depth, 0 = direct column reads
+  int slack_smem;   // 1: slack in shared memory, 0: in registers
+  int ctas_per_sm;  // requested resident chains per SM (0 = as many as fit)
+  int lda_max;
+  size_t smem;
+};
+
+// Validates a batch configuration for models of at most m_max rows and fills
+// rows / smem.  Returns 0 or a naja status code.
+int chr_batch_plan(int m_max, int d, int lda_max, BatchConfig* cfg);
+// Resident CTAs per SM the configuration allows (occupancy calculator).
+int chr_batch_occupancy(const BatchConfig& cfg, int* ctas_per_sm);
+// Persistent launch over nitems (model, chain) work items (device arrays).
+int chr_batch_launch(const ChrArgs& base, const ModelDesc* models, const int* item_model, const int* item_chain,
+                     int nitems, const BatchConfig& cfg, cudaStream_t stream);
+
 // Seeds nchains MRG32k3a states with curand_init(seed, chain_base + c, 0).
 int mrg_init_states(unsigned long long seed, int chain_base, int nchains, void* states, cudaStream_t stream);
 

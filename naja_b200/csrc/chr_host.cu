@@ -18,6 +18,13 @@ int chr_launch_double_256(const ChrArgs& a, int nchains, const ChrLaunchConfig& 
 int chr_launch_double_512(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
 int chr_launch_double_992(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
 
+int chr_batch_dispatch_128(const ChrArgs* base, const ModelDesc* models, const int* im, const int* ic, int nitems,
+                        const BatchConfig& cfg, cudaStream_t stream, int* occ_out);
+int chr_batch_dispatch_256(const ChrArgs* base, const ModelDesc* models, const int* im, const int* ic, int nitems,
+                        const BatchConfig& cfg, cudaStream_t stream, int* occ_out);
+int chr_batch_dispatch_512(const ChrArgs* base, const ModelDesc* models, const int* im, const int* ic, int nitems,
+                        const BatchConfig& cfg, cudaStream_t stream, int* occ_out);
+
 using namespace chr_detail;
 namespace {
 __global__ void mrg_tape_kernel(unsigned long long seed, int chain_base, int nchains, long count, double* tape) {
@@ -98,6 +105,45 @@ int mrg_init_states(unsigned long long seed, int chain_base, int nchains, void* 
   mrg_init_kernel<<<(nchains + 63) / 64, 64, 0, stream>>>(seed, chain_base, nchains,
                                                          static_cast<curandStateMRG32k3a*>(states));
   return cudaGetLastError() == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
+}
+
+int chr_batch_plan(int m_max, int d, int lda_max, BatchConfig* cfg) {
+  const int nt = cfg->threads;
+  if (nt != 128 && nt != 256 && nt != 512) return NAJA_ERR_INVALID_ARGUMENT;
+  int rows = 16;
+  while (rows * nt < m_max) rows *= 2;
+  if (cfg->slack_smem) {
+    if (rows > 64) return NAJA_ERR_UNSUPPORTED;
+  } else if (!((nt == 512 && rows == 16) || (nt == 256 && rows == 32))) {
+    return NAJA_ERR_UNSUPPORTED;
+  }
+  if (cfg->slots != 0 && (cfg->slots < 2 || cfg->slots > kMaxSlots)) return NAJA_ERR_INVALID_ARGUMENT;
+  cfg->rows = rows;
+  cfg->lda_max = lda_max;
+  const Layout L = make_layout(d, lda_max, 4, nt, cfg->slots, cfg->slack_smem ? lda_max : 0);
+  if (L.total > kSmemBudget) return NAJA_ERR_UNSUPPORTED;
+  cfg->smem = L.total;
+  return NAJA_OK;
+}
+
+static int batch_dispatch(const ChrArgs* base, const ModelDesc* models, const int* im, const int* ic, int nitems,
+                          const BatchConfig& cfg, cudaStream_t stream, int* occ) {
+  switch (cfg.threads) {
+    case 128: return chr_batch_dispatch_128(base, models, im, ic, nitems, cfg, stream, occ);
+    case 256: return chr_batch_dispatch_256(base, models, im, ic, nitems, cfg, stream, occ);
+    case 512: return chr_batch_dispatch_512(base, models, im, ic, nitems, cfg, stream, occ);
+    default: return NAJA_ERR_UNSUPPORTED;
+  }
+}
+
+int chr_batch_occupancy(const BatchConfig& cfg, int* ctas_per_sm) {
+  return batch_dispatch(nullptr, nullptr, nullptr, nullptr, 0, cfg, nullptr, ctas_per_sm);
+}
+
+int chr_batch_launch(const ChrArgs& base, const ModelDesc* models, const int* item_model, const int* item_chain,
+                     int nitems, const BatchConfig& cfg, cudaStream_t stream) {
+  if (nitems <= 0) return NAJA_OK;
+  return batch_dispatch(&base, models, item_model, item_chain, nitems, cfg, stream, nullptr);
 }
 
 size_t mrg_state_bytes() { return sizeof(curandStateMRG32k3a); }

@@ -82,12 +82,15 @@ constexpr int kMaxSlots = 8;
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
-  size_t x_off, slot_off, slot_bytes, meta_off, full_off, empty_off, red_off, flag_off, total;
+  size_t x_off, slot_off, slot_bytes, meta_off, full_off, empty_off, red_off, flag_off, slack_off, total;
   int slots;
   bool direct;
 };
 
-__host__ __device__ inline Layout make_layout(int d, int lda, int elt, int nthreads, int slots_req) {
+// slack_rows > 0 reserves a shared-memory slack store (slack_rows values of
+// `elt` bytes) for kernels that keep slack on chip outside the registers.
+__host__ __device__ inline Layout make_layout(int d, int lda, int elt, int nthreads, int slots_req,
+                                              int slack_rows = 0) {
   Layout L;
   const int nw = nthreads / 32;
   const bool direct = slots_req <= 0;
@@ -108,6 +111,8 @@ __host__ __device__ inline Layout make_layout(int d, int lda, int elt, int nthre
   off = align_up(off + sizeof(RedEntry) * 2 * nw, 16);
   L.flag_off = off;
   off += 16;
+  L.slack_off = align_up(off, 128);
+  if (slack_rows > 0) off = L.slack_off + static_cast<size_t>(slack_rows) * elt;
   L.total = align_up(off, 128);
   L.slots = S;
   L.direct = direct;
@@ -437,7 +442,10 @@ __device__ __noinline__ void producer_entry(const ChrArgs& a, const Layout& L, u
   }
 }
 
-template <class Real, int NT, int R>
+// SS: slack in shared memory (row r of this chain at slack[r]) instead of
+// the consumer threads' registers; used by the batched kernel so that several
+// chains share an SM without register pressure.
+template <class Real, int NT, int R, bool SS = false>
 __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* smem, int chain_local) {
   using T = Tier<Real>;
   using Key = typename T::Key;
@@ -457,7 +465,12 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
   for (int j = tid; j < d; j += NT) xs[j] = a.X0[static_cast<size_t>(chain_local) * a.ldx + j];
   named_bar_sync(1, NT);
 
-  Real sl[R];
+  Real sl_reg[SS ? 1 : R];
+  Real* sl_sm = reinterpret_cast<Real*>(smem + L.slack_off) + tid;
+  auto SL = [&](int k) -> Real& {
+    if constexpr (SS) return sl_sm[k * NT];
+    else return sl_reg[k];
+  };
   auto recompute = [&]() {
 #pragma unroll
     for (int k = 0; k < R; ++k) {
@@ -466,9 +479,9 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
         double acc = 0.0;
         const double* Ar = a.A64 + r;
         for (int j = 0; j < d; ++j) acc = __fma_rn(Ar[static_cast<size_t>(j) * lda], xs[j], acc);
-        sl[k] = T::from64(__dsub_rn(a.b[r], acc));
-      } else {
-        sl[k] = Real(0);
+        SL(k) = T::from64(__dsub_rn(a.b[r], acc));
+      } else if constexpr (!SS) {
+        SL(k) = Real(0);  // the shared-memory store holds only rows < m
       }
     }
   };
@@ -530,7 +543,7 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
       for (int k = 0; k < R; ++k) {
         const int r = tid + k * NT;
         if (r < m) {
-          const Key kv = T::key(T::ratio(ae_at(r), sl[k]));
+          const Key kv = T::key(T::ratio(ae_at(r), SL(k)));
           kmax = kv > kmax ? kv : kmax;
           kmin = kv < kmin ? kv : kmin;
         }
@@ -628,7 +641,7 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
 #pragma unroll
       for (int k = 0; k < R; ++k) {
         const int r = tid + k * NT;
-        if (r < m) sl[k] = T::slack_update(sl[k], alpha, ae_at(r));
+        if (r < m) SL(k) = T::slack_update(SL(k), alpha, ae_at(r));
       }
     });
     __syncwarp();
