@@ -10,6 +10,7 @@ from __future__ import annotations
 
 import itertools
 
+from ._lib import NajaError
 from .batch import Batch, Shape
 
 _cache: dict = {}
@@ -22,10 +23,11 @@ CTAS = (0, 1, 2, 3, 4)
 def candidates(batch: Batch):
     seen = set()
     for t, s, ss, c in itertools.product(THREADS, SLOTS, (1, 0), CTAS):
-        if ss == 0 and t == 128:
-            continue
         shape = Shape(t, s, ss, c)
-        occ = batch.occupancy(shape)
+        try:
+            occ = batch.occupancy(shape)
+        except NajaError:  # no instantiated capacity holds these models
+            continue
         if occ == 0:
             continue
         eff = (t, s, ss, min(c, occ) if c else occ)

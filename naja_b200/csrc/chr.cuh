@@ -47,7 +47,7 @@ struct ChrArgs {
 
 struct ChrLaunchConfig {
   int threads;    // consumer threads per chain (multiple of 32)
-  int rows;       // rows held per consumer thread (template capacity)
+  int rows;       // row chunks held per consumer warp (template capacity)
   int slots;      // staged-column ring depth (0 = read columns straight from L2/HBM)
   size_t smem;    // dynamic shared memory bytes
 };
@@ -85,13 +85,25 @@ struct ModelDesc {
 
 struct BatchConfig {
   int threads;      // consumer threads per chain
-  int rows;         // rows per consumer thread (template capacity)
+  int rows;         // row chunks per consumer warp (template capacity)
   int slots;        // ring depth, 0 = direct column reads
   int slack_smem;   // 1: slack in shared memory, 0: in registers
   int ctas_per_sm;  // requested resident chains per SM (0 = as many as fit)
   int lda_max;
   size_t smem;
 };
+
+// Chunk-per-warp capacities instantiated for the batched kernel, per
+// (consumer threads, slack store), ascending; 0 ends a list.
+inline const int* batch_chunk_capacities(int threads, bool slack_smem) {
+  static const int k512s[] = {4, 8, 0}, k512r[] = {4, 8, 0};
+  static const int k256s[] = {4, 8, 16, 0}, k256r[] = {6, 8, 12, 0};
+  static const int k128s[] = {12, 16, 0}, k128r[] = {12, 16, 0};
+  if (threads == 512) return slack_smem ? k512s : k512r;
+  if (threads == 256) return slack_smem ? k256s : k256r;
+  if (threads == 128) return slack_smem ? k128s : k128r;
+  return nullptr;
+}
 
 // Validates a batch configuration for models of at most m_max rows and fills
 // rows / smem.  Returns 0 or a naja status code.

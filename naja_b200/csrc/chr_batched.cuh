@@ -18,46 +18,50 @@ namespace chr_detail {
 namespace {
 
 template <int NT, int R, bool SS>
-__global__ void __launch_bounds__(NT + 32, SS ? (NT <= 256 ? 3 : 2) : 1)
-    chr_batched_kernel(ChrArgs base, const ModelDesc* __restrict__ models, const int* __restrict__ item_model,
-                       const int* __restrict__ item_chain, int nitems, int slots, int lda_max) {
+__global__ void __launch_bounds__(NT + 32, NT >= 512 ? 2 : (NT == 256 ? 3 : 4))
+    chr_batched_kernel(const __grid_constant__ ChrArgs base, const __grid_constant__ Layout L,
+                       const ModelDesc* __restrict__ models, const int* __restrict__ item_model,
+                       const int* __restrict__ item_chain, int nitems) {
   using Real = float;
   extern __shared__ __align__(128) unsigned char smem[];
-  const Layout L = make_layout(base.d, lda_max, sizeof(Real), NT, slots, SS ? lda_max : 0);
+  // The current item's arguments: shared memory rather than a local copy,
+  // which the out-of-line producer call would force onto the stack.
+  __shared__ ChrArgs item_args;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);
   uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.flag_off);
   if (threadIdx.x == 0) *abort_flag = 0;
   for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const int ch = item_chain[item];
     if (threadIdx.x == 0) {
       for (int s = 0; s < L.slots; ++s) {
         mbar_init(&full[s], 1);
         mbar_init(&empty[s], NT / 32);
       }
       fence_mbar_init();
+      const ModelDesc& md = models[item_model[item]];
+      ChrArgs a = base;
+      a.A32 = md.A32;
+      a.A64 = md.A64;
+      a.lda = md.lda;
+      a.m = md.m;
+      a.b = md.b;
+      a.X0 = md.X0;
+      a.ldx = md.ldx;
+      a.samples = md.samples;
+      a.X_final = md.X_final;
+      a.seed = md.seed;
+      a.chain_base = 0;
+      a.rng_state = nullptr;
+      a.wait_cycles = nullptr;
+      item_args = a;
     }
     __syncthreads();
     if (*abort_flag) break;  // every thread reads it after the barrier
-    const int mi = item_model[item], ch = item_chain[item];
-    const ModelDesc md = models[mi];
-    ChrArgs a = base;
-    a.A32 = md.A32;
-    a.A64 = md.A64;
-    a.lda = md.lda;
-    a.m = md.m;
-    a.b = md.b;
-    a.X0 = md.X0;
-    a.ldx = md.ldx;
-    a.samples = md.samples;
-    a.X_final = md.X_final;
-    a.seed = md.seed;
-    a.chain_base = 0;
-    a.rng_state = nullptr;
-    a.wait_cycles = nullptr;
     if (threadIdx.x >= NT) {
-      if (threadIdx.x == NT) producer_entry<Real>(a, L, smem, ch);
+      if (threadIdx.x == NT) producer_entry<Real>(item_args, L, smem, ch);
     } else {
-      run_consumers<Real, NT, R, SS>(a, L, smem, ch);
+      run_consumers<Real, NT, R, kBatchV, SS, false, false>(item_args, L, smem, ch);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -83,7 +87,8 @@ int batch_launch_one(const ChrArgs& base, const ModelDesc* models, const int* im
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int per_sm = cfg.ctas_per_sm > 0 ? (cfg.ctas_per_sm < occ ? cfg.ctas_per_sm : occ) : occ;
   const int grid = nitems < sms * per_sm ? nitems : sms * per_sm;
-  kern<<<grid, NT + 32, cfg.smem, stream>>>(base, models, im, ic, nitems, cfg.slots, cfg.lda_max);
+  const Layout L = make_layout(base.d, cfg.lda_max, sizeof(float), NT, cfg.slots, SS ? cfg.lda_max : 0);
+  kern<<<grid, NT + 32, cfg.smem, stream>>>(base, L, models, im, ic, nitems);
   return cudaGetLastError() == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
 }
 
@@ -96,7 +101,8 @@ int batch_occupancy_one(const BatchConfig& cfg, int* out) {
   return e == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
 }
 
-// Dispatch over the instantiated (rows, slack store) pairs of one thread count.
+// Dispatch over the instantiated (chunks per warp, slack store) pairs of one
+// thread count.
 template <int NT>
 int batch_dispatch(const ChrArgs* base, const ModelDesc* models, const int* im, const int* ic, int nitems,
                    const BatchConfig& cfg, cudaStream_t stream, int* occ_out) {
@@ -104,14 +110,24 @@ int batch_dispatch(const ChrArgs* base, const ModelDesc* models, const int* im, 
   if (cfg.rows == RR && cfg.slack_smem == (SSV ? 1 : 0))                                    \
     return occ_out ? batch_occupancy_one<NT, RR, SSV>(cfg, occ_out)                         \
                    : batch_launch_one<NT, RR, SSV>(*base, models, im, ic, nitems, cfg, stream);
-  NAJA_BATCH_CASE(16, true)
-  NAJA_BATCH_CASE(32, true)
-  NAJA_BATCH_CASE(64, true)
+  // The capacities listed in batch_chunk_capacities (chr.cuh).
   if constexpr (NT == 512) {
+    NAJA_BATCH_CASE(4, true)
+    NAJA_BATCH_CASE(8, true)
+    NAJA_BATCH_CASE(4, false)
+    NAJA_BATCH_CASE(8, false)
+  } else if constexpr (NT == 256) {
+    NAJA_BATCH_CASE(4, true)
+    NAJA_BATCH_CASE(8, true)
+    NAJA_BATCH_CASE(16, true)
+    NAJA_BATCH_CASE(6, false)
+    NAJA_BATCH_CASE(8, false)
+    NAJA_BATCH_CASE(12, false)
+  } else {
+    NAJA_BATCH_CASE(12, true)
+    NAJA_BATCH_CASE(16, true)
+    NAJA_BATCH_CASE(12, false)
     NAJA_BATCH_CASE(16, false)
-  }
-  if constexpr (NT == 256) {
-    NAJA_BATCH_CASE(32, false)
   }
 #undef NAJA_BATCH_CASE
   return NAJA_ERR_UNSUPPORTED;

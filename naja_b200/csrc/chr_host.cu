@@ -40,7 +40,9 @@ __global__ void mrg_init_kernel(unsigned long long seed, int chain_base, int nch
   if (c < nchains) curand_init(seed, static_cast<unsigned long long>(chain_base + c), 0ull, &st[c]);
 }
 
-int max_rows_for(int threads) { return threads <= 512 ? 32 : 16; }
+// Largest chunks-per-warp capacity instantiated for a thread count (the
+// slack of R chunks takes R * kStandaloneV registers per thread).
+int max_chunks_for(int threads) { return threads <= 512 ? 16 : 8; }
 
 }  // namespace
 
@@ -58,9 +60,11 @@ int chr_plan(int precision, int m, int d, int lda, int tpb, int max_slots, ChrLa
     while (threads < 512 && (m + threads - 1) / threads > 8) threads *= 2;
     if ((m + threads - 1) / threads > 8) threads = 992;
   }
+  const int chunk = 32 * kStandaloneV;
+  const int chunks = (m + chunk - 1) / chunk, warps = threads / 32;
   int rows = 1;
-  while (rows * threads < m) rows *= 2;
-  if (rows > max_rows_for(threads)) return NAJA_ERR_UNSUPPORTED;
+  while (rows * warps < chunks) rows *= 2;
+  if (rows > max_chunks_for(threads)) return NAJA_ERR_UNSUPPORTED;
   int slots = kMaxSlots;
   if (max_slots > 0 && max_slots < slots) slots = max_slots;
   Layout L = make_layout(d, lda, elt, threads, slots);
@@ -110,18 +114,21 @@ int mrg_init_states(unsigned long long seed, int chain_base, int nchains, void* 
 int chr_batch_plan(int m_max, int d, int lda_max, BatchConfig* cfg) {
   const int nt = cfg->threads;
   if (nt != 128 && nt != 256 && nt != 512) return NAJA_ERR_INVALID_ARGUMENT;
-  int rows = 16;
-  while (rows * nt < m_max) rows *= 2;
-  if (cfg->slack_smem) {
-    if (rows > 64) return NAJA_ERR_UNSUPPORTED;
-  } else if (!((nt == 512 && rows == 16) || (nt == 256 && rows == 32))) {
-    return NAJA_ERR_UNSUPPORTED;
+  const int chunks = (m_max + 32 * kBatchV - 1) / (32 * kBatchV), warps = nt / 32;
+  int rows = 0;
+  for (const int* c = batch_chunk_capacities(nt, cfg->slack_smem != 0); *c; ++c) {
+    if (*c * warps >= chunks) {
+      rows = *c;
+      break;
+    }
   }
+  if (rows == 0) return NAJA_ERR_UNSUPPORTED;
   if (cfg->slots != 0 && (cfg->slots < 2 || cfg->slots > kMaxSlots)) return NAJA_ERR_INVALID_ARGUMENT;
   cfg->rows = rows;
   cfg->lda_max = lda_max;
   const Layout L = make_layout(d, lda_max, 4, nt, cfg->slots, cfg->slack_smem ? lda_max : 0);
-  if (L.total > kSmemBudget) return NAJA_ERR_UNSUPPORTED;
+  // the kernel also holds one ChrArgs in static shared memory
+  if (L.total + align_up(sizeof(ChrArgs), 128) > kSmemBudget) return NAJA_ERR_UNSUPPORTED;
   cfg->smem = L.total;
   return NAJA_OK;
 }

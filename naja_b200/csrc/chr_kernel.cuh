@@ -15,9 +15,11 @@
 //     A columns those steps need into a ring of shared-memory slots with
 //     1-D bulk copies (cp.async.bulk) that complete on per-slot mbarriers.
 //     The consumers find the column already on chip.
-//   * The slack vector lives in the consumers' registers (thread t owns rows
-//     t, t+NT, ...), so the only memory traffic per step is one column of A
-//     (two for a pair step) plus the amortised sample write.
+//   * The slack vector lives in the consumers' registers (warp w owns the
+//     32 V-row chunks w, w + NW, ..., lane l the V consecutive rows at
+//     l V of each), so the only memory traffic per step is one column of A
+//     (two for a pair step) plus the amortised sample write, read with
+//     vector accesses.
 //   * max/min run on the integer reduction unit (redux.sync) over
 //     order-preserving keys, then across warps through a double-buffered
 //     shared array and one named barrier per step: exact in any order.
@@ -43,16 +45,22 @@ namespace naja {
 namespace chr_detail {
 namespace {
 
+// One step's record in the ring.  The first 32 bytes are what the FP32 tier
+// reads every step (two 16-byte loads): the direction, and its coefficients
+// and alpha uniform rounded to float once by the producer.
 struct __align__(16) StepMeta {
   int kind;
   int ei;
   int ej;
   int slot_b;
+  int k;
+  float cif;
+  float cjf;
+  float uf;
   double ci;
   double cj;
   double u;
-  int k;
-  int pad;
+  double pad;
   int ks_idx[32];
   double ks_coef[32];
 };
@@ -72,6 +80,7 @@ struct StepDir {
 struct RedEntry {
   unsigned long long kmax;
   unsigned long long kmin;
+  unsigned long long kmin2;
   int abort;
   int pad;
 };
@@ -82,7 +91,7 @@ constexpr int kMaxSlots = 8;
 __host__ __device__ inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 struct Layout {
-  size_t x_off, slot_off, slot_bytes, meta_off, full_off, empty_off, red_off, flag_off, slack_off, total;
+  size_t x_off, slot_off, slot_bytes, meta_off, full_off, empty_off, red_off, flag_off, tail_off, slack_off, total;
   int slots;
   bool direct;
 };
@@ -111,6 +120,10 @@ __host__ __device__ inline Layout make_layout(int d, int lda, int elt, int nthre
   off = align_up(off + sizeof(RedEntry) * 2 * nw, 16);
   L.flag_off = off;
   off += 16;
+  // slack of the rows of the partial chunk at the end of the rows (at most
+  // one chunk of 32 * 4 values) when the full chunks keep theirs in registers
+  L.tail_off = align_up(off, 16);
+  off = L.tail_off + 128 * static_cast<size_t>(elt);
   L.slack_off = align_up(off, 128);
   if (slack_rows > 0) off = L.slack_off + static_cast<size_t>(slack_rows) * elt;
   L.total = align_up(off, 128);
@@ -242,22 +255,52 @@ struct Tier<float> {
   __device__ static float ks_acc(float acc, float av, double coef) {
     return __fmaf_rn(av, static_cast<float>(coef), acc);
   }
-  // Ratio ae/s with the reference's special cases; a negative FP32 slack
-  // counts as 0 (it can only come from FP32 rounding).
-  // With s clamped to +0 the IEEE quotient is already the reference's
-  // s == 0 rule (ae/+0 = +-inf, 0/0 = NaN -> 0), so no branch is needed.
-  // A zero numerator is answered without dividing (the IEEE result: +-0 for
-  // s > 0, NaN -> 0 for s = +0): most rows of a sparse A are zero and a
-  // division of zero leaves the division's fast path.
+  // Ratio ae/s of the FP32 tier: a negative slack counts as 0 (it can only
+  // come from FP32 rounding), so a nonzero ae over zero slack is +-inf (the
+  // reference's s == 0 rule, chr.cu:420-429), and a zero ae gives +0 whatever
+  // the slack.  A nonzero ae over a finite slack >= +0 is never NaN.  The
+  // zero numerator is replaced by 1 before dividing: most rows of a sparse A
+  // are zero and a division of zero leaves the division's fast path.
+  // The clamp is one signed-integer max on the bit pattern: every value with
+  // the sign bit set, -0 included, becomes +0.
   __device__ static float ratio(float ae, float s) {
-    s = (s <= 0.0f) ? 0.0f : s;
+    s = __int_as_float(max(__float_as_int(s), 0));
     const bool z = (ae == 0.0f);
-    const float q = __fdiv_rn(z ? 1.0f : ae, z ? 1.0f : s);
-    return z ? ((s > 0.0f) ? ae : 0.0f) : ((q != q) ? 0.0f : q);
+    const float q = __fdiv_rn(z ? 1.0f : ae, s);
+    return z ? 0.0f : q;
   }
-  __device__ static float alpha(float mx, float mn, double u) {
+  // Running extremes on the raw bit patterns (ratios are never NaN), exact
+  // in the key order -0 < +0 without transforming each value:
+  //   hi  = signed-integer max: the largest ratio whenever some ratio has a
+  //         clear sign bit (integer order is float order there, and every
+  //         such value is above every value with the sign bit set);
+  //   lo  = unsigned max: the most negative ratio whenever some ratio has its
+  //         sign bit set (the magnitude grows with the unsigned value);
+  //   lo2 = unsigned min: the largest ratio when all have the sign bit set
+  //         (smallest magnitude), the smallest when none has.
+  using Acc = uint32_t;
+  __device__ static Acc acc_hi0() { return 0x80000000u; }
+  __device__ static Acc acc_lo0() { return 0u; }
+  __device__ static Acc acc_lo20() { return 0xffffffffu; }
+  __device__ static void acc(Acc& hi, Acc& lo, Acc& lo2, float v) {
+    const uint32_t b = __float_as_uint(v);
+    hi = static_cast<uint32_t>(max(static_cast<int>(hi), static_cast<int>(b)));
+    lo = max(lo, b);
+    lo2 = min(lo2, b);
+  }
+  __device__ static Acc red_hi(Acc v) {
+    return static_cast<uint32_t>(__reduce_max_sync(0xffffffffu, static_cast<int>(v)));
+  }
+  __device__ static Acc red_lo(Acc v) { return __reduce_max_sync(0xffffffffu, v); }
+  __device__ static Acc red_lo2(Acc v) { return __reduce_min_sync(0xffffffffu, v); }
+  __device__ static void decode(Acc hi, Acc lo, Acc lo2, float& mx, float& mn) {
+    mx = __uint_as_float(static_cast<int>(hi) >= 0 ? hi : lo2);
+    mn = __uint_as_float(lo >= 0x80000000u ? lo : lo2);
+  }
+  using UType = float;
+  __device__ static float alpha(float mx, float mn, float u) {
     const float lo = __fdiv_rn(1.0f, mn), hi = __fdiv_rn(1.0f, mx);
-    return __fmaf_rn(static_cast<float>(u), __fsub_rn(hi, lo), lo);
+    return __fmaf_rn(u, __fsub_rn(hi, lo), lo);
   }
   __device__ static double coef(double c) { return static_cast<double>(static_cast<float>(c)); }
   __device__ static float slack_update(float s, float alpha, float ae) { return __fmaf_rn(-alpha, ae, s); }
@@ -294,12 +337,32 @@ struct Tier<double> {
   __device__ static double ks_acc(double acc, double av, double coef) { return __fma_rn(av, coef, acc); }
   // s == 0 of either sign becomes +0: ae/+0 = +-inf, 0/0 = NaN -> 0, the
   // reference's rule (chr.cu:420-429); negative slack divides as it is.
+  // A nonzero ae over a finite slack is never NaN, so the NaN -> 0 rule only
+  // concerns 0/0, answered by the zero-numerator branch.
   __device__ static double ratio(double ae, double s) {
     s = (s == 0.0) ? 0.0 : s;
     const bool z = (ae == 0.0);
     const double q = __ddiv_rn(z ? 1.0 : ae, z ? 1.0 : s);
-    return z ? ((s > 0.0) ? ae : ((s < 0.0) ? -ae : 0.0)) : ((q != q) ? 0.0 : q);
+    return z ? ((s > 0.0) ? ae : ((s < 0.0) ? -ae : 0.0)) : q;
   }
+  // Extremes over order-preserving keys (exact in any order); lo2 unused.
+  using Acc = unsigned long long;
+  __device__ static Acc acc_hi0() { return dkey(lowest()); }
+  __device__ static Acc acc_lo0() { return dkey(highest()); }
+  __device__ static Acc acc_lo20() { return 0ull; }
+  __device__ static void acc(Acc& hi, Acc& lo, Acc&, double v) {
+    const Acc kv = dkey(v);
+    hi = kv > hi ? kv : hi;
+    lo = kv < lo ? kv : lo;
+  }
+  __device__ static Acc red_hi(Acc v) { return wmax(v); }
+  __device__ static Acc red_lo(Acc v) { return wmin(v); }
+  __device__ static Acc red_lo2(Acc v) { return v; }
+  __device__ static void decode(Acc hi, Acc lo, Acc, double& mx, double& mn) {
+    mx = dkey_inv(hi);
+    mn = dkey_inv(lo);
+  }
+  using UType = double;
   __device__ static double alpha(double mx, double mn, double u) {
     const double lo = __ddiv_rn(1.0, mn), hi = __ddiv_rn(1.0, mx);
     return __fma_rn(u, __dsub_rn(hi, lo), lo);
@@ -380,6 +443,9 @@ __device__ __noinline__ void run_producer(const ChrArgs& a, Src& src, const Layo
     M.cj = dir.cj;
     M.u = dir.u;
     M.k = dir.k;
+    M.cif = static_cast<float>(dir.ci);
+    M.cjf = static_cast<float>(dir.cj);
+    M.uf = static_cast<float>(dir.u);
     if (dir.kind == kKSparse) {
       for (int q = 0; q < dir.k; ++q) {
         M.ks_idx[q] = ks_idx[q];
@@ -442,14 +508,71 @@ __device__ __noinline__ void producer_entry(const ChrArgs& a, const Layout& L, u
   }
 }
 
+// V consecutive values through 16-byte (or narrower) vector accesses; the
+// address is a multiple of V elements.
+template <class Real, int V>
+__device__ __forceinline__ void vload(const Real* p, Real (&o)[V]) {
+  if constexpr (sizeof(Real) == 4 && V % 4 == 0) {
+#pragma unroll
+    for (int i = 0; i < V; i += 4) {
+      const float4 q = *reinterpret_cast<const float4*>(p + i);
+      o[i] = q.x;
+      o[i + 1] = q.y;
+      o[i + 2] = q.z;
+      o[i + 3] = q.w;
+    }
+  } else if constexpr (sizeof(Real) == 4 && V == 2) {
+    const float2 q = *reinterpret_cast<const float2*>(p);
+    o[0] = q.x;
+    o[1] = q.y;
+  } else if constexpr (sizeof(Real) == 8 && V % 2 == 0) {
+#pragma unroll
+    for (int i = 0; i < V; i += 2) {
+      const double2 q = *reinterpret_cast<const double2*>(p + i);
+      o[i] = q.x;
+      o[i + 1] = q.y;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < V; ++i) o[i] = p[i];
+  }
+}
+
+template <class Real, int V>
+__device__ __forceinline__ void vstore(Real* p, const Real (&v)[V]) {
+  if constexpr (sizeof(Real) == 4 && V % 4 == 0) {
+#pragma unroll
+    for (int i = 0; i < V; i += 4) *reinterpret_cast<float4*>(p + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+  } else if constexpr (sizeof(Real) == 4 && V == 2) {
+    *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+  } else if constexpr (sizeof(Real) == 8 && V % 2 == 0) {
+#pragma unroll
+    for (int i = 0; i < V; i += 2) *reinterpret_cast<double2*>(p + i) = make_double2(v[i], v[i + 1]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < V; ++i) p[i] = v[i];
+  }
+}
+
+// Consumer side of one chain.
+//
+// Rows are handed out in chunks of C = 32 V rows: chunk c covers rows
+// [c C, c C + C), lane l of the owning warp holds rows c C + l V + [0, V)
+// and reads them with one vector access.  Warp w owns chunks w, w + NW, ...
+// (at most R of them).  Every chunk test is uniform across the warp, so
+// rows past m cost nothing; only the one partial chunk at the end of the
+// rows tests each row.
+//
 // SS: slack in shared memory (row r of this chain at slack[r]) instead of
 // the consumer threads' registers; used by the batched kernel so that several
 // chains share an SM without register pressure.
-template <class Real, int NT, int R, bool SS = false>
+template <class Real, int NT, int R, int V, bool SS = false, bool TIMING = true, bool MAYBE_DIRECT = true>
 __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* smem, int chain_local) {
   using T = Tier<Real>;
-  using Key = typename T::Key;
+  using Acc = typename T::Acc;
+  using UT = typename T::UType;
   constexpr int NW = NT / 32;
+  constexpr int C = 32 * V;
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
   double* xs = reinterpret_cast<double*>(smem + L.x_off);
@@ -461,29 +584,86 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
   const Real* A = T::A(a);
   const int m = a.m, d = a.d, lda = a.lda, S = L.slots;
   const int gchain = a.chain_base + chain_local;
+  const bool direct = MAYBE_DIRECT && L.direct;
+  // This warp's chunks: full ones at k < my_full, then (for one warp) the
+  // partial chunk at k == my_full.
+  const int n_full = m / C;
+  const int my_full = n_full > warp ? (n_full - warp + NW - 1) / NW : 0;
+  const bool my_tail = (m % C) != 0 && (n_full % NW) == warp;
+  const int base0 = warp * C + lane * V;
 
   for (int j = tid; j < d; j += NT) xs[j] = a.X0[static_cast<size_t>(chain_local) * a.ldx + j];
   named_bar_sync(1, NT);
 
-  Real sl_reg[SS ? 1 : R];
-  Real* sl_sm = reinterpret_cast<Real*>(smem + L.slack_off) + tid;
-  auto SL = [&](int k) -> Real& {
-    if constexpr (SS) return sl_sm[k * NT];
-    else return sl_reg[k];
-  };
-  auto recompute = [&]() {
+  // Calls full(k, base) for each full chunk of this warp (k, the chunk's
+  // index in the warp, is a constant once the loop is unrolled; base is the
+  // lane's first row), then tail(base) for the partial chunk if this warp
+  // owns it.
+  const int tail_base = base0 + my_full * NW * C;
+  auto for_chunks = [&](auto&& full_fn, auto&& tail_fn) {
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-      const int r = tid + k * NT;
-      if (r < m) {
-        double acc = 0.0;
-        const double* Ar = a.A64 + r;
-        for (int j = 0; j < d; ++j) acc = __fma_rn(Ar[static_cast<size_t>(j) * lda], xs[j], acc);
-        SL(k) = T::from64(__dsub_rn(a.b[r], acc));
-      } else if constexpr (!SS) {
-        SL(k) = Real(0);  // the shared-memory store holds only rows < m
-      }
+      if (k >= my_full) break;
+      full_fn(k, base0 + k * NW * C);
     }
+    if (my_tail) tail_fn(tail_base);
+  };
+
+  Real sl_reg[SS ? 1 : R * V];
+  Real* sl_sm = reinterpret_cast<Real*>(smem + L.slack_off);
+  auto slack_get = [&](int k, int base, Real (&s)[V]) {
+    if constexpr (SS) {
+      vload<Real, V>(sl_sm + base, s);
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v) s[v] = sl_reg[k * V + v];
+    }
+  };
+  auto slack_put = [&](int k, int base, const Real (&s)[V]) {
+    if constexpr (SS) {
+      vstore<Real, V>(sl_sm + base, s);
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v) sl_reg[k * V + v] = s[v];
+    }
+  };
+  // Slack of row r of the partial chunk.
+  Real* tail_sl = reinterpret_cast<Real*>(smem + L.tail_off) - n_full * C;
+  auto slack_tail = [&](int r) -> Real& {
+    if constexpr (SS) return sl_sm[r];
+    else return tail_sl[r];
+  };
+
+  auto recompute = [&]() {
+    for_chunks(
+        [&](int k, int base) {
+          double acc[V];
+#pragma unroll
+          for (int v = 0; v < V; ++v) acc[v] = 0.0;
+          const double* Ar = a.A64 + base;
+          for (int j = 0; j < d; ++j) {
+            const double xj = xs[j];
+            const double* Aj = Ar + static_cast<size_t>(j) * lda;
+#pragma unroll
+            for (int v = 0; v < V; ++v) acc[v] = __fma_rn(Aj[v], xj, acc[v]);
+          }
+          Real s[V];
+#pragma unroll
+          for (int v = 0; v < V; ++v) s[v] = T::from64(__dsub_rn(a.b[base + v], acc[v]));
+          slack_put(k, base, s);
+        },
+        [&](int base) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const int r = base + v;
+            if (r < m) {
+              double acc = 0.0;
+              const double* Ar = a.A64 + r;
+              for (int j = 0; j < d; ++j) acc = __fma_rn(Ar[static_cast<size_t>(j) * lda], xs[j], acc);
+              slack_tail(r) = T::from64(__dsub_rn(a.b[r], acc));
+            }
+          }
+        });
   };
   recompute();
 
@@ -495,24 +675,38 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
   int thin_ctr = 0, resync_ctr = 0, rbuf = 0;
   size_t out_row = static_cast<size_t>(gchain);
   unsigned long long w_full = 0;
-  const unsigned long long c_start = clock64();
+  const unsigned long long c_start = TIMING ? clock64() : 0ull;
   for (long long t = 0; t < total; ++t) {
     const int sa = slot;
-    const unsigned long long w0 = a.wait_cycles ? clock64() : 0ull;
+    const unsigned long long w0 = (TIMING && a.wait_cycles) ? clock64() : 0ull;
     bool ok = mbar_wait_bounded(&full[sa], parity, a.timeout_ns);
-    if (a.wait_cycles) w_full += clock64() - w0;
+    if (TIMING && a.wait_cycles) w_full += clock64() - w0;
     int kind = kCoord, ei = 0, ej = 0, sb = -1, kq = 0;
-    double ci = 1.0, cj = 0.0, u = 0.5;
+    Real cir = Real(1), cjr = Real(0);
+    UT uu = UT(0.5);
+    double cix = 1.0, cjx = 0.0;  // the coefficients as the x update uses them
     if (ok) {
       const StepMeta& M = meta[sa];
-      kind = M.kind;
-      ei = M.ei;
-      ej = M.ej;
-      sb = M.slot_b;
-      ci = M.ci;
-      cj = M.cj;
-      u = M.u;
-      kq = M.k;
+      const int4 h0 = *reinterpret_cast<const int4*>(&M.kind);
+      const int4 h1 = *reinterpret_cast<const int4*>(&M.k);
+      kind = h0.x;
+      ei = h0.y;
+      ej = h0.z;
+      sb = h0.w;
+      kq = h1.x;
+      if constexpr (sizeof(Real) == 4) {
+        cir = __int_as_float(h1.y);
+        cjr = __int_as_float(h1.z);
+        uu = __int_as_float(h1.w);
+        cix = static_cast<double>(cir);
+        cjx = static_cast<double>(cjr);
+      } else {
+        cir = M.ci;
+        cjr = M.cj;
+        uu = M.u;
+        cix = cir;
+        cjx = cjr;
+      }
       if (++slot == S) {
         slot = 0;
         parity ^= 1u;
@@ -533,25 +727,10 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
       }
       if (++resync_ctr == a.resync) resync_ctr = 0;
     }
-    Key kmax = T::key(T::lowest()), kmin = T::key(T::highest());
     // Row passes, specialised once per step on the (warp-uniform) kind and
     // on where the column lives, so the per-row code is straight-line.
     // ae = A u for row r is evaluated identically in the ratio pass and the
     // slack update (the slot stays resident until the step releases it).
-    auto scan = [&](auto ae_at) {
-#pragma unroll
-      for (int k = 0; k < R; ++k) {
-        const int r = tid + k * NT;
-        if (r < m) {
-          const Key kv = T::key(T::ratio(ae_at(r), SL(k)));
-          kmax = kv > kmax ? kv : kmax;
-          kmin = kv < kmin ? kv : kmin;
-        }
-      }
-    };
-    const Real cir = static_cast<Real>(ci), cjr = static_cast<Real>(cj);
-    const Real* gca = A + static_cast<size_t>(ei) * lda;
-    const Real* gcb = A + static_cast<size_t>(ej) * lda;
     const Real* sca = reinterpret_cast<const Real*>(smem + L.slot_off + static_cast<size_t>(sa) * L.slot_bytes);
     const Real* scb = reinterpret_cast<const Real*>(smem + L.slot_off +
                                                     static_cast<size_t>(sb < 0 ? 0 : sb) * L.slot_bytes);
@@ -561,64 +740,103 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
       for (int q = 0; q < kq; ++q) acc = T::ks_acc(acc, A[r + static_cast<size_t>(M.ks_idx[q]) * lda], M.ks_coef[q]);
       return acc;
     };
-    auto for_kind = [&](auto pass) {
+    // pass(vec, one): vec(base, ae[V]) fills a full chunk's V values, one(r)
+    // returns row r's value.
+    auto for_kind = [&](auto&& pass) {
       if (kind == kCoord) {
-        if (L.direct) pass([&](int r) -> Real { return gca[r]; });
-        else pass([&](int r) -> Real { return sca[r]; });
+        const Real* col = direct ? A + static_cast<size_t>(ei) * lda : sca;
+        pass([&](int base, Real(&o)[V]) { vload<Real, V>(col + base, o); }, [&](int r) -> Real { return col[r]; });
       } else if (kind == kPair) {
-        if (L.direct) pass([&](int r) -> Real { return T::pair_ae_r(gca[r], gcb[r], cir, cjr); });
-        else pass([&](int r) -> Real { return T::pair_ae_r(sca[r], scb[r], cir, cjr); });
+        const Real* ca = direct ? A + static_cast<size_t>(ei) * lda : sca;
+        const Real* cb = direct ? A + static_cast<size_t>(ej) * lda : scb;
+        pass(
+            [&](int base, Real(&o)[V]) {
+              Real x1[V], x2[V];
+              vload<Real, V>(ca + base, x1);
+              vload<Real, V>(cb + base, x2);
+#pragma unroll
+              for (int v = 0; v < V; ++v) o[v] = T::pair_ae_r(x1[v], x2[v], cir, cjr);
+            },
+            [&](int r) -> Real { return T::pair_ae_r(ca[r], cb[r], cir, cjr); });
       } else {
-        pass(ks_at);
+        pass(
+            [&](int base, Real(&o)[V]) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) o[v] = ks_at(base + v);
+            },
+            ks_at);
       }
     };
-    if (ok) for_kind([&](auto ae_at) { scan(ae_at); });
-    kmax = T::wmax(kmax);
-    kmin = T::wmin(kmin);
+    // Cross-warp combination of (hi, lo, lo2): lane 0 of each warp posts its
+    // warp's values; after one barrier lane l of every warp picks up warp l's
+    // entry and a second warp reduction yields the chain's.  The two halves
+    // of `red` alternate between consecutive steps.
+    Acc hi = T::acc_hi0(), lo = T::acc_lo0(), lo2 = T::acc_lo20();
+    if (ok) {
+      for_kind([&](auto&& vec, auto&& one) {
+        for_chunks(
+            [&](int k, int base) {
+              Real ae[V], s[V];
+              vec(base, ae);
+              slack_get(k, base, s);
+#pragma unroll
+              for (int v = 0; v < V; ++v) T::acc(hi, lo, lo2, T::ratio(ae[v], s[v]));
+            },
+            [&](int base) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) {
+                const int r = base + v;
+                if (r < m) T::acc(hi, lo, lo2, T::ratio(one(r), slack_tail(r)));
+              }
+            });
+      });
+    }
+    hi = T::red_hi(hi);
+    lo = T::red_lo(lo);
+    lo2 = T::red_lo2(lo2);
     if (NW > 1) {
-      // Lane 0 of each warp posts its warp's extremes; after one barrier lane
-      // l of every warp picks up warp l's entry and a second warp reduction
-      // yields the block's.  Double-buffered: step t+1 writes the other half.
       RedEntry* slotr = red + rbuf * NW;
       rbuf ^= 1;
       const int bad = __any_sync(0xffffffffu, !ok) ? 1 : 0;
       if (lane == 0) {
-        slotr[warp].kmax = kmax;
-        slotr[warp].kmin = kmin;
+        slotr[warp].kmax = hi;
+        slotr[warp].kmin = lo;
+        slotr[warp].kmin2 = lo2;
         slotr[warp].abort = bad;
       }
       named_bar_sync(1, NT);
-      Key k1 = T::key(T::lowest()), k2 = T::key(T::highest());
-      int b = 0;
+      Acc h = T::acc_hi0(), l = T::acc_lo0(), l2 = T::acc_lo20();
+      int bflag = 0;
       if (lane < NW) {
-        k1 = static_cast<Key>(slotr[lane].kmax);
-        k2 = static_cast<Key>(slotr[lane].kmin);
-        b = slotr[lane].abort;
+        h = static_cast<Acc>(slotr[lane].kmax);
+        l = static_cast<Acc>(slotr[lane].kmin);
+        l2 = static_cast<Acc>(slotr[lane].kmin2);
+        bflag = slotr[lane].abort;
       }
-      kmax = T::wmax(k1);
-      kmin = T::wmin(k2);
-      if (__any_sync(0xffffffffu, b)) {
-        if (tid == 0) {
-          set_error(a.err, kDevTimeoutFull, sa, static_cast<int>(parity), static_cast<int>(t));
-          *abort_flag = 1;
-        }
-        return;
-      }
-    } else if (__any_sync(0xffffffffu, !ok)) {
-      if (lane == 0) {
+      hi = T::red_hi(h);
+      lo = T::red_lo(l);
+      lo2 = T::red_lo2(l2);
+      ok = !__any_sync(0xffffffffu, bflag);
+    } else {
+      ok = !__any_sync(0xffffffffu, !ok);
+    }
+    if (!ok) {
+      if (tid == 0) {
         set_error(a.err, kDevTimeoutFull, sa, static_cast<int>(parity), static_cast<int>(t));
         *abort_flag = 1;
       }
       return;
     }
-    const Real alpha = T::alpha(T::unkey(kmax), T::unkey(kmin), u);
+    Real mx, mn;
+    T::decode(hi, lo, lo2, mx, mn);
+    const Real alpha = T::alpha(mx, mn, uu);
     const double a64 = static_cast<double>(alpha);
     // x update: entry j belongs to consumer thread j % NT.
     if (kind == kCoord) {
       if (ei % NT == tid) xs[ei] = __dadd_rn(xs[ei], a64);
     } else if (kind == kPair) {
-      if (ei % NT == tid) xs[ei] = __fma_rn(a64, T::coef(ci), xs[ei]);
-      if (ej % NT == tid) xs[ej] = __fma_rn(a64, T::coef(cj), xs[ej]);
+      if (ei % NT == tid) xs[ei] = __fma_rn(a64, cix, xs[ei]);
+      if (ej % NT == tid) xs[ej] = __fma_rn(a64, cjx, xs[ej]);
     } else {
       const StepMeta& M = meta[sa];
       for (int q = 0; q < kq; ++q) {
@@ -637,12 +855,23 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
       out_row += static_cast<size_t>(a.out_nchains);
     }
     if (++thin_ctr == a.thinning) thin_ctr = 0;
-    for_kind([&](auto ae_at) {
+    for_kind([&](auto&& vec, auto&& one) {
+      for_chunks(
+          [&](int k, int base) {
+            Real ae[V], s[V];
+            vec(base, ae);
+            slack_get(k, base, s);
 #pragma unroll
-      for (int k = 0; k < R; ++k) {
-        const int r = tid + k * NT;
-        if (r < m) SL(k) = T::slack_update(SL(k), alpha, ae_at(r));
-      }
+            for (int v = 0; v < V; ++v) s[v] = T::slack_update(s[v], alpha, ae[v]);
+            slack_put(k, base, s);
+          },
+          [&](int base) {
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+              const int r = base + v;
+              if (r < m) slack_tail(r) = T::slack_update(slack_tail(r), alpha, one(r));
+            }
+          });
     });
     __syncwarp();
     if (lane == 0) {
@@ -653,16 +882,24 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
   if (a.X_final) {
     for (int j = tid; j < d; j += NT) a.X_final[static_cast<size_t>(chain_local) * a.ldx + j] = xs[j];
   }
-  if (a.wait_cycles && tid == 0) {
+  if (TIMING && a.wait_cycles && tid == 0) {
     a.wait_cycles[4 * chain_local + 0] = w_full;
     a.wait_cycles[4 * chain_local + 2] = clock64() - c_start;
   }
 }
 
+// Rows per lane per chunk of the single-model kernel: 8- (FP32) or 16-byte
+// (FP64) vector accesses, 64-row chunks; shorter chunks spread a model's rows
+// evenly over many warps, which bounds the latency of one step.
+constexpr int kStandaloneV = 2;
+// The batched kernel (FP32 only) runs several chains per SM and is bound by
+// instruction issue, so it takes 16-byte accesses: 128-row chunks.
+constexpr int kBatchV = 4;
+
 template <class Real, int NT, int R>
-__global__ void __launch_bounds__(NT + 32, 1) chr_kernel(ChrArgs a, int slots) {
+__global__ void __launch_bounds__(NT + 32, 1)
+    chr_kernel(const __grid_constant__ ChrArgs a, const __grid_constant__ Layout L) {
   extern __shared__ __align__(128) unsigned char smem[];
-  const Layout L = make_layout(a.d, a.lda, sizeof(Real), NT, slots);
   const int chain_local = blockIdx.x;
   if (threadIdx.x == 0) {
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);
@@ -679,7 +916,7 @@ __global__ void __launch_bounds__(NT + 32, 1) chr_kernel(ChrArgs a, int slots) {
     if (threadIdx.x == NT) producer_entry<Real>(a, L, smem, chain_local);
     return;
   }
-  run_consumers<Real, NT, R>(a, L, smem, chain_local);
+  run_consumers<Real, NT, R, kStandaloneV>(a, L, smem, chain_local);
 }
 
 // ------------------------------------------------------------- dispatch
@@ -688,10 +925,12 @@ int launch_one(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaSt
   auto kern = chr_kernel<Real, NT, R>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(cfg.smem));
   if (e != cudaSuccess) return NAJA_ERR_CUDA;
-  kern<<<nchains, NT + 32, cfg.smem, stream>>>(a, cfg.slots);
+  const Layout L = make_layout(a.d, a.lda, sizeof(Real), NT, cfg.slots);
+  kern<<<nchains, NT + 32, cfg.smem, stream>>>(a, L);
   return cudaGetLastError() == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
 }
 
+// cfg.rows = chunks per warp (template capacity).
 template <class Real, int NT>
 int launch_rows(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream) {
   switch (cfg.rows) {
@@ -699,9 +938,8 @@ int launch_rows(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaS
     case 2: return launch_one<Real, NT, 2>(a, nchains, cfg, stream);
     case 4: return launch_one<Real, NT, 4>(a, nchains, cfg, stream);
     case 8: return launch_one<Real, NT, 8>(a, nchains, cfg, stream);
-    case 16: return launch_one<Real, NT, 16>(a, nchains, cfg, stream);
-    case 32:
-      if constexpr (NT <= 512) return launch_one<Real, NT, 32>(a, nchains, cfg, stream);
+    case 16:
+      if constexpr (NT <= 512) return launch_one<Real, NT, 16>(a, nchains, cfg, stream);
       break;
     default: break;
   }

@@ -25,7 +25,8 @@
  *                written as explicit fma() at the points nvcc contracts in
  *                the reference build (-fmad defaults to true there).
  *   precision=0  the FP32 tier of the new sampler: FP32 A copy, FP32 slack
- *                with negative slack treated as 0 in the ratio, FP32 ratios
+ *                with negative slack treated as 0 in the ratio, a zero
+ *                numerator giving the ratio +0 for any slack, FP32 ratios
  *                and alpha, FP64 position x, FP64 slack recompute
  *                (b - A64*x64, sequential fma over columns) every
  *                resync_interval steps.
@@ -340,11 +341,12 @@ static int run_chain(const run_cfg* c, int chain, draw_src* src, uint64_t step_o
                 const float ae = ae32(c, &dir, r);
                 aes32[r] = ae;
                 float inv;
-                if (s == 0.0f) {
-                    inv = (ae > 0.0f) ? INFINITY : ((ae < 0.0f) ? -INFINITY : 0.0f);
+                if (ae == 0.0f) {
+                    inv = 0.0f; /* the FP32 tier's zero numerator: +0 */
+                } else if (s == 0.0f) {
+                    inv = (ae > 0.0f) ? INFINITY : -INFINITY;
                 } else {
                     inv = ae / s;
-                    if (isnan(inv)) inv = 0.0f;
                 }
                 uint32_t kv = key32(inv);
                 if (kv > kmax) kmax = kv;
