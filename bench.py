@@ -316,6 +316,8 @@ def _ours(a, rank, world):
         line["cpu_baseline"] = _cpu_baseline(W, a, min_ess / W.steps)
     if rank == 0 and a.batch_models > 0:
         line["batched"] = _batched(a, torch, dev)
+    if rank == 0 and a.learned_train > 0:
+        line["learned_rounding"] = _learned(a)
     P.close()
     return line
 
@@ -404,6 +406,22 @@ def _batched(a, torch, dev):
                          "peak_source": src, "bytes_per_chr_step": bytes_total / steps},
             "autotune_top": sorted(({"shape": str(k), "M_steps_per_s": v / 1e6} for k, v in table.items()),
                                    key=lambda r: -r["M_steps_per_s"])[:5]}
+
+
+def _learned(a):
+    """Learned vs Dikin vs plain CHR on held-out conditioned variants of the
+    genome-shaped polytope (the batched-variant generator): the rounding
+    network is trained on the project's kernels from covariance factors of
+    plain-CHR samples of the training variants (training time reported
+    separately); each method then samples the held-out variants in one
+    batched launch, 8 chains x 1000 samples, thinning 116, pair-prob 0.3;
+    min-ESS (chain-summed, y-space) per variant over its share of the
+    sampling + rounding-map time."""
+    from naja_b200 import learned
+
+    return learned.run_experiment(n=a.n, d=a.d, n_train=a.learned_train, n_test=a.learned_test,
+                                  nchains=8, nspc_train=500, nspc_test=1000, thinning=a.thinning,
+                                  pair_prob=a.pair_prob, epochs=a.learned_epochs, resync=a.resync, seed=a.seed)
 
 
 def _reference_arm(a, rank, world):
@@ -515,6 +533,10 @@ def main(argv=None):
                     help="reference arm: time budget of the K timed steps")
     ap.add_argument("--ref-cpu", action="store_true", help="reference arm: time the CPU restatement")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--learned-train", type=int, default=256,
+                    help="learned-rounding section: training variants (0 = skip)")
+    ap.add_argument("--learned-test", type=int, default=16)
+    ap.add_argument("--learned-epochs", type=int, default=60)
     a = ap.parse_args(argv)
     if a.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

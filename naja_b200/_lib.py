@@ -1,4 +1,5 @@
-"""ctypes binding of libnaja_b200.so (the C ABI in include/naja_chr.h).
+"""ctypes binding of libnaja_b200.so (the C ABI in include/naja_chr.h and
+include/naja_mlp.h).
 
 There is no fallback: if the shared library is missing or a symbol is
 absent, loading raises.  Build it with `python -m naja_b200.build`.
@@ -51,6 +52,33 @@ EXPORTED = (
     "naja_graph_check",
     "naja_graph_destroy",
 )
+
+# Every entry point include/naja_mlp.h declares.
+EXPORTED_MLP = (
+    "naja_gemm_bf16",
+    "naja_mlp_check",
+    "naja_cast_bf16",
+    "naja_gelu_backward",
+    "naja_mse_grad",
+    "naja_col_sum",
+    "naja_adam",
+)
+
+
+class GemmEpilogue(C.Structure):
+    """Mirror of `naja_gemm_epilogue`."""
+
+    _fields_ = [
+        ("bias", C.c_void_p),
+        ("c_f32", C.c_void_p),
+        ("ldc", C.c_int),
+        ("accumulate", C.c_int),
+        ("act", C.c_void_p),
+        ("ld_act", C.c_int),
+        ("act_t", C.c_void_p),
+        ("ld_act_t", C.c_int),
+        ("gelu", C.c_int),
+    ]
 
 
 class ChrParams(C.Structure):
@@ -112,7 +140,7 @@ def load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(f"{LIB_PATH} is missing: build it with `python -m naja_b200.build`")
     lib = C.CDLL(str(LIB_PATH))
-    for name in EXPORTED:
+    for name in EXPORTED + EXPORTED_MLP:
         if not hasattr(lib, name):
             raise ImportError(f"{LIB_PATH} does not export {name}")
     vp, i, ll, d, ull = C.c_void_p, C.c_int, C.c_longlong, C.c_double, C.c_ulonglong
@@ -140,6 +168,16 @@ def load() -> C.CDLL:
     lib.naja_graph_launch.argtypes = [vp, vp]
     lib.naja_graph_check.argtypes = [vp]
     lib.naja_graph_destroy.argtypes = [vp]
+    f = C.c_float
+    lib.naja_gemm_bf16.argtypes = [i, i, i, vp, i, vp, i, C.POINTER(GemmEpilogue), vp]
+    lib.naja_mlp_check.argtypes = [vp]
+    lib.naja_cast_bf16.argtypes = [i, i, vp, i, vp, i, vp, i, vp]
+    lib.naja_gelu_backward.argtypes = [i, i, vp, vp, i, vp, vp, i, vp, i, vp]
+    lib.naja_mse_grad.argtypes = [i, i, vp, vp, i, vp, vp, vp, vp, i, vp, i, vp]
+    lib.naja_col_sum.argtypes = [i, i, vp, i, vp, vp]
+    lib.naja_adam.argtypes = [i, i, vp, vp, vp, vp, i, f, f, f, f, i, vp, i, vp, i, vp]
+    for name in EXPORTED_MLP:
+        getattr(lib, name).restype = C.c_int
     for name in EXPORTED:
         f = getattr(lib, name)
         if f.restype is C.c_int or name in ("naja_polytope_create", "naja_polytope_destroy", "naja_polytope_shape",

@@ -43,6 +43,7 @@ def _units():
     units.append(("validate", CSRC / "validate.cu", ["-fmad=false"]))
     units.append(("backmap", CSRC / "backmap.cu", ["-fmad=false"]))
     units.append(("backmap_tc", CSRC / "backmap_tc.cu", []))
+    units.append(("mlp", CSRC / "mlp.cu", []))
     return units
 
 
@@ -96,7 +97,30 @@ def build(jobs: int | None = None, force: bool = False, verbose: bool = False) -
             raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}{r.stderr}")
         os.replace(tmp, LIB)
         link_stamp.write_text(h.hexdigest())
+    _build_cli(force)
     return LIB
+
+
+CLI_SRC = PKG / "cli" / "naja_cli.cpp"
+CLI = PKG / "bin" / "naja"
+
+
+def _build_cli(force: bool = False) -> Path:
+    """The `naja` command line (host C++ over the C ABI), linked to the
+    in-tree library through an $ORIGIN-relative rpath."""
+    cmd = ["/usr/bin/g++", "-O2", "-std=c++17", "-Wall", "-I", str(ROOT / "include"), str(CLI_SRC), "-L", str(PKG),
+           "-lnaja_b200", "-Wl,-rpath,$ORIGIN/..", "-o", str(CLI)]
+    stamp = OUT / "cli.sha256"
+    h = hashlib.sha256(" ".join(cmd).encode())
+    h.update(CLI_SRC.read_bytes())
+    h.update((ROOT / "include" / "naja_chr.h").read_bytes())
+    if force or not CLI.exists() or not stamp.exists() or stamp.read_text() != h.hexdigest():
+        CLI.parent.mkdir(exist_ok=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"g++ failed:\n{' '.join(cmd)}\n{r.stdout}{r.stderr}")
+        stamp.write_text(h.hexdigest())
+    return CLI
 
 
 def main(argv=None):

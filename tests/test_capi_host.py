@@ -11,8 +11,8 @@ from naja_b200 import _lib, synth
 ROOT = Path(__file__).resolve().parent.parent
 
 
-def _declared_functions():
-    text = (ROOT / "include" / "naja_chr.h").read_text()
+def _declared_functions(header="naja_chr.h"):
+    text = (ROOT / "include" / header).read_text()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(naja_[a-z0-9_]+)\s*\(", text)))
 
@@ -24,6 +24,17 @@ def test_library_exports_every_declared_symbol():
     for name in declared:
         assert hasattr(lib, name), name
     assert set(declared) == set(_lib.EXPORTED)
+    mlp = _declared_functions("naja_mlp.h")
+    assert "naja_gemm_bf16" in mlp
+    for name in mlp:
+        assert hasattr(lib, name), name
+    assert set(mlp) == set(_lib.EXPORTED_MLP)
+
+
+def test_gemm_epilogue_struct_layout():
+    E = _lib.GemmEpilogue
+    assert E.c_f32.offset == 8 and E.act.offset == 24 and E.act_t.offset == 40 and E.gelu.offset == 52
+    assert C.sizeof(E) == 56
 
 
 def test_params_default_matches_reference_defaults():
