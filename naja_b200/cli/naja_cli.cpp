@@ -1,0 +1,829 @@
+// `naja` command line: the sampling and validate commands of quothbonney/naja
+// over this project's C ABI (include/naja_chr.h).
+//
+//   naja sample run --model-dir DIR --out-root DIR --n-chains K --n-samples S [flags]
+//       src/cli/sample/cmd_run.cpp:44-237 (flags, checks, phase lines) and
+//       src/engine/job_sampling.cu:82-445 (the job): model-directory contract
+//       (src/pipeline/model_contract.cpp:56-84), run directory
+//       <out-root>/<model>_<YYYYMMDD>_<NNN> (model_contract.cpp:217-230),
+//       config_generated.txt, run_manifest.json (src/pipeline/run_manifest.cpp:
+//       74-143), samples.npy as (n_samples, dim) float32 C order with the
+//       reference's header padding (src/npy.h:96-141), profile.json
+//       (src/engine/profile.h:28-66), config_used.txt (job_sampling.cu:34-60).
+//       Thinning defaults to max(d/6, 1) and the seed to the reference's hash
+//       of model name, model directory and GPU (job_sampling.cu:237-254).
+//   naja validate --samples F.npy [--model-dir DIR] [--n-chains 4]
+//       src/cli/validate_cli.cpp:49-296: ESS / split-R-hat (naja_validate, the
+//       reference's chain windows), bounds compliance of v = T y + shift
+//       against the GEM bounds (src/validate/bounds_check.cpp:8-39), the
+//       one-line status to stderr and the JSON report to stdout.
+//
+// Flags the reference accepts for features this project leaves out
+// (iterative rounding passes, affine-hull reduction, the cube-centre start
+// LP) are rejected with a usage error instead of being ignored.
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <functional>
+#include <iomanip>
+#include <iostream>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/naja_chr.h"
+
+namespace {
+
+// ------------------------------------------------------------------ files
+bool path_exists(const std::string& p) {
+  struct stat st;
+  return stat(p.c_str(), &st) == 0;
+}
+bool is_directory(const std::string& p) {
+  struct stat st;
+  return stat(p.c_str(), &st) == 0 && S_ISDIR(st.st_mode);
+}
+void ensure_dir(const std::string& p) {
+  if (p.empty() || is_directory(p)) return;
+  const auto slash = p.find_last_of('/');
+  if (slash != std::string::npos && slash > 0) ensure_dir(p.substr(0, slash));
+  if (mkdir(p.c_str(), 0755) != 0 && !is_directory(p)) throw std::runtime_error("cannot create directory: " + p);
+}
+std::string absolute(const std::string& p) {
+  if (p.empty()) return p;
+  char buf[4096];
+  if (realpath(p.c_str(), buf)) return buf;
+  if (p[0] == '/') return p;
+  if (getcwd(buf, sizeof(buf))) return std::string(buf) + "/" + p;
+  return p;
+}
+std::string stamp(const char* fmt) {
+  const std::time_t now = std::time(nullptr);
+  char b[64];
+  std::strftime(b, sizeof(b), fmt, std::localtime(&now));
+  return b;
+}
+std::string self_path() {
+  char buf[4096];
+  const ssize_t n = readlink("/proc/self/exe", buf, sizeof(buf) - 1);
+  if (n <= 0) return "naja";
+  buf[n] = 0;
+  return buf;
+}
+
+// CSV of numbers; rows separated by newlines, values by commas.
+struct Csv {
+  int rows = 0, cols = 0;
+  std::vector<double> v;  // row-major
+};
+Csv load_csv(const std::string& path) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f.is_open()) throw std::runtime_error("cannot open file: " + path);
+  std::string text((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+  Csv c;
+  const char* p = text.c_str();
+  const char* end = p + text.size();
+  while (p < end) {
+    const char* eol = static_cast<const char*>(std::memchr(p, '\n', end - p));
+    if (!eol) eol = end;
+    int cols = 0;
+    const char* q = p;
+    bool any = false;
+    for (const char* s = p; s < eol; ++s)
+      if (!std::isspace(static_cast<unsigned char>(*s))) any = true;
+    if (any) {
+      while (q < eol) {
+        char* next = nullptr;
+        const double x = std::strtod(q, &next);
+        if (next == q) throw std::runtime_error("bad number in " + path + " at row " + std::to_string(c.rows + 1));
+        c.v.push_back(x);
+        ++cols;
+        q = next;
+        while (q < eol && (*q == ' ' || *q == '\t' || *q == '\r')) ++q;
+        if (q < eol && *q == ',') ++q;
+        while (q < eol && (*q == ' ' || *q == '\t' || *q == '\r')) ++q;
+      }
+      if (c.rows == 0) c.cols = cols;
+      else if (cols != c.cols) throw std::runtime_error("ragged csv: " + path);
+      ++c.rows;
+    }
+    p = eol + 1;
+  }
+  if (c.rows == 0) throw std::runtime_error("empty csv: " + path);
+  return c;
+}
+// Column-major copy (rows x cols, ld = rows).
+std::vector<double> colmajor(const Csv& c) {
+  std::vector<double> out(static_cast<size_t>(c.rows) * c.cols);
+  for (int r = 0; r < c.rows; ++r)
+    for (int k = 0; k < c.cols; ++k) out[static_cast<size_t>(k) * c.rows + r] = c.v[static_cast<size_t>(r) * c.cols + k];
+  return out;
+}
+
+// (rows, cols) float32 C order, header as src/npy.h:96-141 writes it.
+void save_npy_f32(const std::string& path, const float* data, long long rows, long long cols) {
+  std::ofstream f(path, std::ios::binary);
+  if (!f.is_open()) throw std::runtime_error("Cannot write file: " + path);
+  f.write("\x93NUMPY", 6);
+  f.put(0x01);
+  f.put(0x00);
+  std::ostringstream h;
+  h << "{'descr': '<f4', 'fortran_order': False, 'shape': (" << rows << ", " << cols << "), }";
+  std::string hs = h.str();
+  const size_t total = 6 + 2 + 2 + hs.size();
+  hs.append((64 - total % 64) % 64, ' ');
+  hs.push_back('\n');
+  const uint16_t len = static_cast<uint16_t>(hs.size());
+  f.write(reinterpret_cast<const char*>(&len), 2);
+  f.write(hs.data(), len);
+  f.write(reinterpret_cast<const char*>(data), static_cast<std::streamsize>(rows * cols * sizeof(float)));
+}
+
+// Loads an npy of '<f4' or '<f8' as float32 (rows, cols) C order.
+std::vector<float> load_npy(const std::string& path, long long* rows, long long* cols) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f.is_open()) throw std::runtime_error("cannot open: " + path);
+  char magic[6];
+  f.read(magic, 6);
+  if (std::memcmp(magic, "\x93NUMPY", 6) != 0) throw std::runtime_error("not an npy file: " + path);
+  char ver[2];
+  f.read(ver, 2);
+  uint32_t hlen = 0;
+  if (ver[0] == 1) {
+    uint16_t h16;
+    f.read(reinterpret_cast<char*>(&h16), 2);
+    hlen = h16;
+  } else {
+    f.read(reinterpret_cast<char*>(&hlen), 4);
+  }
+  std::string header(hlen, ' ');
+  f.read(&header[0], hlen);
+  const bool f32 = header.find("'<f4'") != std::string::npos, f64 = header.find("'<f8'") != std::string::npos;
+  if (!f32 && !f64) throw std::runtime_error("unsupported dtype in " + path);
+  if (header.find("'fortran_order': True") != std::string::npos) throw std::runtime_error("fortran order npy: " + path);
+  const auto sp = header.find("'shape':"), p1 = header.find('(', sp), p2 = header.find(')', p1);
+  std::string s = header.substr(p1 + 1, p2 - p1 - 1);
+  std::replace(s.begin(), s.end(), ',', ' ');
+  std::stringstream ss(s);
+  ss >> *rows >> *cols;
+  const size_t n = static_cast<size_t>(*rows) * static_cast<size_t>(*cols);
+  std::vector<float> out(n);
+  if (f32) {
+    f.read(reinterpret_cast<char*>(out.data()), static_cast<std::streamsize>(n * 4));
+  } else {
+    std::vector<double> b(n);
+    f.read(reinterpret_cast<char*>(b.data()), static_cast<std::streamsize>(n * 8));
+    for (size_t i = 0; i < n; ++i) out[i] = static_cast<float>(b[i]);
+  }
+  if (!f) throw std::runtime_error("truncated npy: " + path);
+  return out;
+}
+
+// SHA-256 (FIPS 180-4) of a file, for the run manifest.
+std::string sha256_file(const std::string& path) {
+  static const uint32_t K[64] = {
+      0x428a2f98, 0x71374491, 0xb5c0fbcf, 0xe9b5dba5, 0x3956c25b, 0x59f111f1, 0x923f82a4, 0xab1c5ed5, 0xd807aa98,
+      0x12835b01, 0x243185be, 0x550c7dc3, 0x72be5d74, 0x80deb1fe, 0x9bdc06a7, 0xc19bf174, 0xe49b69c1, 0xefbe4786,
+      0x0fc19dc6, 0x240ca1cc, 0x2de92c6f, 0x4a7484aa, 0x5cb0a9dc, 0x76f988da, 0x983e5152, 0xa831c66d, 0xb00327c8,
+      0xbf597fc7, 0xc6e00bf3, 0xd5a79147, 0x06ca6351, 0x14292967, 0x27b70a85, 0x2e1b2138, 0x4d2c6dfc, 0x53380d13,
+      0x650a7354, 0x766a0abb, 0x81c2c92e, 0x92722c85, 0xa2bfe8a1, 0xa81a664b, 0xc24b8b70, 0xc76c51a3, 0xd192e819,
+      0xd6990624, 0xf40e3585, 0x106aa070, 0x19a4c116, 0x1e376c08, 0x2748774c, 0x34b0bcb5, 0x391c0cb3, 0x4ed8aa4a,
+      0x5b9cca4f, 0x682e6ff3, 0x748f82ee, 0x78a5636f, 0x84c87814, 0x8cc70208, 0x90befffa, 0xa4506ceb, 0xbef9a3f7,
+      0xc67178f2};
+  uint32_t H[8] = {0x6a09e667, 0xbb67ae85, 0x3c6ef372, 0xa54ff53a, 0x510e527f, 0x9b05688c, 0x1f83d9ab, 0x5be0cd19};
+  std::ifstream f(path, std::ios::binary);
+  if (!f.is_open()) return "";
+  std::string data((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+  const uint64_t bits = static_cast<uint64_t>(data.size()) * 8;
+  data.push_back(static_cast<char>(0x80));
+  while (data.size() % 64 != 56) data.push_back(0);
+  for (int i = 7; i >= 0; --i) data.push_back(static_cast<char>((bits >> (8 * i)) & 0xff));
+  auto rotr = [](uint32_t x, int n) { return (x >> n) | (x << (32 - n)); };
+  for (size_t off = 0; off < data.size(); off += 64) {
+    uint32_t w[64];
+    for (int i = 0; i < 16; ++i) {
+      const unsigned char* p = reinterpret_cast<const unsigned char*>(data.data() + off + 4 * i);
+      w[i] = (uint32_t(p[0]) << 24) | (uint32_t(p[1]) << 16) | (uint32_t(p[2]) << 8) | uint32_t(p[3]);
+    }
+    for (int i = 16; i < 64; ++i) {
+      const uint32_t s0 = rotr(w[i - 15], 7) ^ rotr(w[i - 15], 18) ^ (w[i - 15] >> 3);
+      const uint32_t s1 = rotr(w[i - 2], 17) ^ rotr(w[i - 2], 19) ^ (w[i - 2] >> 10);
+      w[i] = w[i - 16] + s0 + w[i - 7] + s1;
+    }
+    uint32_t a = H[0], b = H[1], c = H[2], d = H[3], e = H[4], fv = H[5], g = H[6], h = H[7];
+    for (int i = 0; i < 64; ++i) {
+      const uint32_t S1 = rotr(e, 6) ^ rotr(e, 11) ^ rotr(e, 25);
+      const uint32_t ch = (e & fv) ^ (~e & g);
+      const uint32_t t1 = h + S1 + ch + K[i] + w[i];
+      const uint32_t S0 = rotr(a, 2) ^ rotr(a, 13) ^ rotr(a, 22);
+      const uint32_t mj = (a & b) ^ (a & c) ^ (b & c);
+      const uint32_t t2 = S0 + mj;
+      h = g;
+      g = fv;
+      fv = e;
+      e = d + t1;
+      d = c;
+      c = b;
+      b = a;
+      a = t1 + t2;
+    }
+    H[0] += a;
+    H[1] += b;
+    H[2] += c;
+    H[3] += d;
+    H[4] += e;
+    H[5] += fv;
+    H[6] += g;
+    H[7] += h;
+  }
+  std::ostringstream o;
+  for (uint32_t x : H) o << std::hex << std::setw(8) << std::setfill('0') << x;
+  return o.str();
+}
+
+void json_string(std::ostream& o, const std::string& s) {
+  o << '"';
+  for (char c : s) {
+    if (c == '"' || c == '\\') o << '\\' << c;
+    else if (c == '\n') o << "\\n";
+    else o << c;
+  }
+  o << '"';
+}
+
+void phase(bool on, const std::string& what) {
+  if (on) std::cout << "> " << what << std::endl;
+}
+void kv(bool on, const std::string& k, const std::string& v) {
+  if (on) std::cout << "  " << std::left << std::setw(16) << k << v << std::endl;
+}
+
+void check(int st) {
+  if (st != NAJA_OK) throw std::runtime_error(naja_last_error());
+}
+
+double seconds_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// ------------------------------------------------------------ sample run
+[[noreturn]] void die_usage(const std::string& msg) {
+  std::cerr << "error: " << msg << "\n\nusage:\n"
+            << "  naja sample run --model-dir <dir> --out-root <dir> --n-chains K --n-samples S\n"
+            << "      [--gpu 0] [--tpb 128] [--thinning T] [--pair-prob p] [--resync-interval K]\n"
+            << "      [--ksparse-prob p] [--ksparse-k k] [--extra-constraints auto|ignore|require]\n"
+            << "      [--backmap] [--write-npy] [--bounds-policy ignore|filter] [--bounds-eps e]\n"
+            << "      [--write-samples-valid] [--precision fp32|fp64] [--rng philox|mrg]\n"
+            << "      [--backmap-mode fp64|tf32x3|bf16x3] [--verbose] [--quiet] [--dry-run] [--print-config]\n";
+  std::exit(2);
+}
+
+std::string next_arg(int& i, int argc, char** argv, const std::string& flag) {
+  if (i + 1 >= argc) die_usage("missing value for " + flag);
+  return argv[++i];
+}
+
+struct RunConfig {
+  std::string model_dir, model_name, rounding_dir, gem_dir, data_dir, out_dir;
+  int gpu = 0, n_chains = -1, n_samples = -1, tpb = 128, thinning = 0, resync_interval = 0, ksparse_k = 8;
+  double pair_prob = 0.0, ksparse_prob = 0.0, bounds_eps = 1e-6;
+  std::string extra_constraints = "auto", bounds_policy = "ignore", precision = "fp32", rng = "philox",
+              backmap_mode = "fp64";
+  bool backmap = false, write_npy = false, verbose = false, quiet = false, dry_run = false, print_config = false,
+       write_samples_valid = false;
+  std::string file(const std::string& what) const { return rounding_dir + "/" + model_name + "_rounding_" + what + ".csv"; }
+};
+
+void require_nonempty(const std::string& path, const std::string& what) {
+  struct stat st;
+  if (!path_exists(path)) throw std::runtime_error("missing " + what + ": " + path);
+  if (stat(path.c_str(), &st) != 0) throw std::runtime_error("cannot stat " + what + ": " + path);
+  if (st.st_size == 0) throw std::runtime_error("empty " + what + ": " + path);
+}
+
+void validate_contract(const RunConfig& c) {
+  if (!is_directory(c.rounding_dir)) throw std::runtime_error("missing rounding/ dir: " + c.rounding_dir);
+  require_nonempty(c.file("A"), "rounding_A");
+  require_nonempty(c.file("b"), "rounding_b");
+  require_nonempty(c.file("start"), "rounding_start");
+  if (c.backmap) {
+    require_nonempty(c.file("T"), "rounding_T");
+    require_nonempty(c.file("shift"), "rounding_shift");
+  }
+  const bool ha = path_exists(c.file("extra_A")), hb = path_exists(c.file("extra_b"));
+  if (ha != hb)
+    throw std::runtime_error("extra constraints must be both-present or both-absent: " + c.file("extra_A") + " / " +
+                             c.file("extra_b"));
+  if (ha) {
+    require_nonempty(c.file("extra_A"), "extra_A");
+    require_nonempty(c.file("extra_b"), "extra_b");
+  }
+}
+
+std::string allocate_run_dir(const std::string& out_root, const std::string& name) {
+  ensure_dir(out_root);
+  const std::string date = stamp("%Y%m%d");
+  for (int idx = 1; idx < 1000000; ++idx) {
+    std::ostringstream o;
+    o << out_root << "/" << name << "_" << date << "_" << std::setw(3) << std::setfill('0') << idx;
+    if (!path_exists(o.str())) {
+      ensure_dir(o.str());
+      return o.str();
+    }
+  }
+  throw std::runtime_error("could not allocate run directory under " + out_root);
+}
+
+void write_generated_config(const std::string& path, const RunConfig& c) {
+  std::ofstream f(path);
+  if (!f.is_open()) throw std::runtime_error("cannot write generated config: " + path);
+  f << "DATA_DIR=" << c.data_dir << "\n"
+    << "MODEL_NAME=" << c.model_name << "\n"
+    << "OUT_DIR=" << c.out_dir << "\n"
+    << "N_CHAINS=" << c.n_chains << "\n"
+    << "N_SAMPLES=" << c.n_samples << "\n"
+    << "TPB_SS=" << c.tpb << "\n"
+    << "GPU_DEVICE=" << c.gpu << "\n"
+    << "THINNING=" << c.thinning << "\n"
+    << "PAIR_PROB=" << std::setprecision(17) << c.pair_prob << "\n"
+    << "RESYNC_INTERVAL=" << c.resync_interval << "\n"
+    << "KSPARSE_PROB=" << c.ksparse_prob << "\n"
+    << "KSPARSE_K=" << c.ksparse_k << "\n"
+    << "EXTRA_CONSTRAINTS=" << c.extra_constraints << "\n"
+    << "BACK_TRANSFORM=" << (c.backmap ? 1 : 0) << "\n"
+    << "WRITE_DATA=" << (c.write_npy ? 1 : 0) << "\n"
+    << "BOUNDS_FILTER=" << (c.bounds_policy == "filter" ? 1 : 0) << "\n"
+    << "BOUNDS_EPS=" << c.bounds_eps << "\n"
+    << "WRITE_SAMPLES_VALID=" << (c.write_samples_valid ? 1 : 0) << "\n"
+    << "PRECISION=" << c.precision << "\n"
+    << "RNG=" << c.rng << "\n"
+    << "BACKMAP_MODE=" << c.backmap_mode << "\n";
+}
+
+void write_run_manifest(const RunConfig& c, const std::vector<std::string>& argv_full) {
+  const std::string exe = self_path();
+  struct stat st {};
+  stat(exe.c_str(), &st);
+  std::ofstream f(c.out_dir + "/run_manifest.json");
+  if (!f.is_open()) throw std::runtime_error("cannot write run manifest: " + c.out_dir + "/run_manifest.json");
+  f << "{\n  \"argv\": [";
+  for (size_t i = 0; i < argv_full.size(); ++i) {
+    if (i) f << ", ";
+    json_string(f, argv_full[i]);
+  }
+  f << "],\n  \"model_dir\": ";
+  json_string(f, absolute(c.model_dir));
+  f << ",\n  \"engine\": {\n    \"path\": ";
+  json_string(f, absolute(exe));
+  f << ",\n    \"sha256\": ";
+  json_string(f, sha256_file(exe));
+  f << ",\n    \"size\": " << static_cast<long long>(st.st_size) << ",\n    \"library\": ";
+  json_string(f, naja_version());
+  f << "\n  },\n  \"config\": {\n"
+    << "    \"gpu_device\": " << c.gpu << ",\n"
+    << "    \"n_chains\": " << c.n_chains << ",\n"
+    << "    \"n_samples\": " << c.n_samples << ",\n"
+    << "    \"tpb_ss\": " << c.tpb << ",\n"
+    << "    \"back_transform\": " << (c.backmap ? "true" : "false") << ",\n"
+    << "    \"write_data\": " << (c.write_npy ? "true" : "false") << ",\n"
+    << "    \"bounds_policy\": ";
+  json_string(f, c.bounds_policy);
+  f << ",\n    \"bounds_eps\": " << std::setprecision(12) << c.bounds_eps << ",\n"
+    << "    \"write_samples_valid\": " << (c.write_samples_valid ? "true" : "false") << "\n  },\n"
+    << "  \"resolved_paths\": {\n    \"model_dir\": ";
+  json_string(f, absolute(c.model_dir));
+  const char* keys[] = {"A", "b", "start", "T", "shift", "extra_A", "extra_b"};
+  for (const char* k : keys) {
+    f << ",\n    \"" << k << "\": ";
+    json_string(f, absolute(c.file(k)));
+  }
+  f << "\n  }\n}\n";
+}
+
+struct Profile {
+  double load = 0, upload = 0, sampling = 0, download = 0, backtransform = 0, write = 0, total = 0, throughput = 0;
+  int n_chains = 0, n_samples = 0, reduced_dim = 0, original_dim = 0, constraints = 0, thinning = 0;
+};
+
+void write_profile(const std::string& path, const Profile& p, const RunConfig& c) {
+  std::ofstream f(path);
+  if (!f.is_open()) throw std::runtime_error("cannot write profile: " + path);
+  f << "{\n  \"timestamp\": \"" << stamp("%Y-%m-%d %H:%M:%S") << "\",\n  \"config\": {\n"
+    << "    \"n_chains\": " << p.n_chains << ",\n    \"n_samples\": " << p.n_samples << ",\n"
+    << "    \"reduced_dim\": " << p.reduced_dim << ",\n    \"original_dim\": " << p.original_dim << ",\n"
+    << "    \"constraints\": " << p.constraints << ",\n    \"thinning\": " << p.thinning << ",\n"
+    << "    \"tpb_ss\": " << c.tpb << ",\n    \"gpu_device\": " << c.gpu << ",\n"
+    << "    \"back_transform\": " << (c.backmap ? "true" : "false") << "\n  },\n  \"timing\": {\n"
+    << std::fixed << std::setprecision(4) << "    \"load_polytope_s\": " << p.load << ",\n"
+    << "    \"upload_to_gpu_s\": " << p.upload << ",\n    \"gpu_sampling_s\": " << p.sampling << ",\n"
+    << "    \"download_from_gpu_s\": " << p.download << ",\n    \"backtransform_s\": " << p.backtransform << ",\n"
+    << "    \"write_output_s\": " << p.write << ",\n    \"total_s\": " << p.total << "\n  },\n"
+    << "  \"performance\": {\n    \"total_samples\": " << static_cast<long long>(p.n_chains) * p.n_samples << ",\n"
+    << "    \"throughput_samples_per_sec\": " << std::setprecision(1) << p.throughput << ",\n"
+    << "    \"sampling_fraction\": " << std::setprecision(3) << (p.total > 0 ? p.sampling / p.total : 0.0) << "\n"
+    << "  }\n}\n";
+}
+
+void write_config_used(const RunConfig& c, const std::string& gen) {
+  std::ofstream dst(c.out_dir + "/config_used.txt");
+  std::ifstream src(gen);
+  if (!dst.is_open() || !src.is_open()) throw std::runtime_error("cannot write config snapshot: " + c.out_dir);
+  dst << "# Source config: " << absolute(gen) << "\n# Captured at: " << stamp("%Y-%m-%d %H:%M:%S") << "\n"
+      << "# Output directory: " << absolute(c.out_dir) << "\n\n"
+      << src.rdbuf() << "\n# Derived metadata\nMODEL_NAME=" << c.model_name << "\n"
+      << "DATA_DIR_ABS=" << absolute(c.data_dir) << "\nMODEL_DIR_ABS=" << absolute(c.model_dir) << "\n"
+      << "A_FILE=" << absolute(c.file("A")) << "\nB_FILE=" << absolute(c.file("b")) << "\n";
+}
+
+int run_sampling(const RunConfig& c) {
+  const auto t_total = std::chrono::steady_clock::now();
+  Profile prof;
+  const bool st = !c.quiet;
+  phase(st, "loading polytope");
+  auto t0 = std::chrono::steady_clock::now();
+  Csv A = load_csv(c.file("A")), b = load_csv(c.file("b")), x0 = load_csv(c.file("start"));
+  const bool have_extra = path_exists(c.file("extra_A"));
+  if (c.extra_constraints == "require" && !have_extra)
+    throw std::runtime_error("--extra-constraints require: missing " + c.file("extra_A"));
+  if (have_extra && c.extra_constraints != "ignore") {
+    // append extra rows (src/pipeline/extra_constraints.cpp:17-58)
+    Csv eA = load_csv(c.file("extra_A")), eb = load_csv(c.file("extra_b"));
+    if (eA.cols != A.cols) throw std::runtime_error("extra_A has " + std::to_string(eA.cols) + " columns, A has " + std::to_string(A.cols));
+    if (eb.rows * eb.cols != eA.rows) throw std::runtime_error("extra_b length does not match extra_A rows");
+    A.v.insert(A.v.end(), eA.v.begin(), eA.v.end());
+    A.rows += eA.rows;
+    b.v.insert(b.v.end(), eb.v.begin(), eb.v.end());
+    b.rows += eb.rows * eb.cols;
+  }
+  const int m = A.rows, d = A.cols;
+  if (static_cast<int>(b.v.size()) != m) throw std::runtime_error("dimension mismatch: rhs vector size (" + std::to_string(b.v.size()) + ") != rows (" + std::to_string(m) + ")");
+  if (static_cast<int>(x0.v.size()) != d) throw std::runtime_error("start point has " + std::to_string(x0.v.size()) + " values, A has " + std::to_string(d) + " columns");
+  // feasible start (src/validate/feasibility.h:12-35): max(A x0 - b) <= 1e-9
+  double worst = -1e300;
+  for (int r = 0; r < m; ++r) {
+    double s = 0;
+    for (int k = 0; k < d; ++k) s += A.v[static_cast<size_t>(r) * d + k] * x0.v[k];
+    worst = std::max(worst, s - b.v[r]);
+  }
+  if (worst > 1e-9) throw std::runtime_error("infeasible start point: max(A x0 - b) = " + std::to_string(worst));
+  const int thinning = c.thinning > 0 ? c.thinning : std::max(d / 6, 1);
+  prof.load = seconds_since(t0);
+  prof.n_chains = c.n_chains;
+  prof.n_samples = c.n_samples;
+  prof.reduced_dim = d;
+  prof.constraints = m;
+  prof.thinning = thinning;
+  if (c.verbose) {
+    std::cout << "  constraints     " << m << "\n  reduced_dim     " << d << "\n  thinning        " << thinning
+              << "\n  time            " << std::fixed << std::setprecision(3) << prof.load << "s\n\n";
+  }
+  std::hash<std::string> h;
+  int seed = static_cast<int>(h(c.model_name) ^ (h(c.model_dir) << 1) ^
+                              static_cast<uint64_t>(c.gpu * 0x9e3779b9));
+  if (seed == 0) seed = 1;
+
+  phase(st, "uploading to gpu");
+  t0 = std::chrono::steady_clock::now();
+  const std::vector<double> Acm = colmajor(A);
+  naja_polytope* P = nullptr;
+  check(naja_polytope_create(c.gpu, m, d, Acm.data(), m, b.v.data(), &P));
+  std::vector<double> X0(static_cast<size_t>(d) * c.n_chains);
+  for (int k = 0; k < c.n_chains; ++k) std::copy(x0.v.begin(), x0.v.end(), X0.begin() + static_cast<size_t>(k) * d);
+  prof.upload = seconds_since(t0);
+
+  naja_chr_params p;
+  naja_chr_params_default(&p);
+  p.nspc = c.n_samples;
+  p.thinning = thinning;
+  p.nchains = c.n_chains;
+  p.tpb = c.tpb;
+  p.seed = static_cast<unsigned long long>(static_cast<long long>(seed));
+  p.pair_prob = c.pair_prob;
+  p.resync_interval = c.resync_interval;
+  p.ksparse_prob = c.ksparse_prob;
+  p.ksparse_k = c.ksparse_k;
+  p.precision = c.precision == "fp64" ? NAJA_PREC_FP64 : NAJA_PREC_FP32;
+  p.rng = c.rng == "mrg" ? NAJA_RNG_REF_MRG : NAJA_RNG_PHILOX;
+  p.out_dtype = NAJA_DTYPE_F32;
+  const long long N = static_cast<long long>(c.n_samples) * c.n_chains;
+  std::vector<float> Y(static_cast<size_t>(N) * d);
+  phase(st, c.backmap ? "gpu sampling+backmap" : "gpu sampling");
+  t0 = std::chrono::steady_clock::now();
+  int rc = naja_chr_run(P, &p, X0.data(), d, Y.data(), nullptr, nullptr);
+  prof.sampling = seconds_since(t0);
+  naja_polytope_destroy(P);
+  check(rc);
+  std::vector<float> out;
+  long long dim = d;
+  std::vector<double> Tcm, shift, lb, ub;
+  if (c.backmap) {
+    phase(st, "loading transform");
+    Csv T = load_csv(c.file("T")), sh = load_csv(c.file("shift"));
+    if (T.cols != d) throw std::runtime_error("backmap_into: transformation shape mismatch with samples");
+    Tcm = colmajor(T);
+    shift = sh.v;
+    dim = T.rows;
+    prof.original_dim = T.rows;
+    out.resize(static_cast<size_t>(N) * dim);
+    const int mode = c.backmap_mode == "tf32x3" ? NAJA_BACKMAP_TF32X3
+                     : c.backmap_mode == "bf16x3" ? NAJA_BACKMAP_BF16X3 : NAJA_BACKMAP_FP64;
+    t0 = std::chrono::steady_clock::now();
+    check(naja_backmap(T.rows, d, N, Tcm.data(), T.rows, shift.data(), Y.data(), NAJA_DTYPE_F32, out.data(),
+                       NAJA_DTYPE_F32, mode, nullptr));
+    // the reference times the backmap inside the sampling call (job_sampling.cu:313-336)
+    prof.sampling += seconds_since(t0);
+  } else {
+    out.swap(Y);
+  }
+  prof.throughput = prof.sampling > 0 ? static_cast<double>(N) / prof.sampling : 0.0;
+  if (st) std::cout << "> done: " << std::fixed << std::setprecision(1) << prof.sampling << "s, " << std::setprecision(0)
+                    << prof.throughput << " samples/s" << std::endl;
+  if (c.write_npy) {
+    phase(st, "writing npy");
+    t0 = std::chrono::steady_clock::now();
+    save_npy_f32(c.out_dir + "/samples.npy", out.data(), N, dim);
+    prof.write = seconds_since(t0);
+  }
+  if (c.bounds_policy == "filter") {
+    phase(st, "bounds filter (GEM validity)");
+    const Csv l = load_csv(c.gem_dir + "/l_bounds.csv"), u = load_csv(c.gem_dir + "/u_bounds.csv");
+    if (static_cast<long long>(l.v.size()) != dim || static_cast<long long>(u.v.size()) != dim)
+      throw std::runtime_error("GEM bounds length does not match the sample dimension");
+    std::vector<float> valid;
+    long long n_ok = 0;
+    for (long long s = 0; s < N; ++s) {
+      const float* v = out.data() + s * dim;
+      bool ok = true;
+      for (long long i = 0; i < dim && ok; ++i) {
+        const double viol = std::max(l.v[i] - v[i], v[i] - u.v[i]);
+        if (viol - c.bounds_eps > 0.0) ok = false;
+      }
+      if (ok) {
+        ++n_ok;
+        if (c.write_samples_valid) valid.insert(valid.end(), v, v + dim);
+      }
+    }
+    kv(st, "bounds_valid", std::to_string(n_ok) + "/" + std::to_string(N));
+    if (c.write_samples_valid) save_npy_f32(c.out_dir + "/samples_valid.npy", valid.data(), n_ok, dim);
+  }
+  prof.total = seconds_since(t_total);
+  write_profile(c.out_dir + "/profile.json", prof, c);
+  write_config_used(c, c.out_dir + "/config_generated.txt");
+  if (c.verbose) std::cout << "output      :: " << absolute(c.out_dir) << std::endl;
+  return 0;
+}
+
+int cmd_sample_run(int argc, char** argv) {
+  RunConfig c;
+  std::string out_root;
+  for (int i = 0; i < argc; ++i) {
+    const std::string a = argv[i];
+    if (a == "--model-dir") c.model_dir = next_arg(i, argc, argv, a);
+    else if (a == "--out-root") out_root = next_arg(i, argc, argv, a);
+    else if (a == "--gpu") c.gpu = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--n-chains") c.n_chains = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--n-samples") c.n_samples = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--tpb") c.tpb = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--thinning") c.thinning = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--pair-prob") c.pair_prob = std::stod(next_arg(i, argc, argv, a));
+    else if (a == "--resync-interval") c.resync_interval = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--ksparse-prob") c.ksparse_prob = std::stod(next_arg(i, argc, argv, a));
+    else if (a == "--ksparse-k") c.ksparse_k = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--extra-constraints") c.extra_constraints = next_arg(i, argc, argv, a);
+    else if (a == "--backmap") c.backmap = true;
+    else if (a == "--write-npy") c.write_npy = true;
+    else if (a == "--verbose") c.verbose = true;
+    else if (a == "--bounds-policy") c.bounds_policy = next_arg(i, argc, argv, a);
+    else if (a == "--bounds-eps") c.bounds_eps = std::stod(next_arg(i, argc, argv, a));
+    else if (a == "--write-samples-valid") c.write_samples_valid = true;
+    else if (a == "--quiet") c.quiet = true;
+    else if (a == "--dry-run") c.dry_run = true;
+    else if (a == "--print-config") c.print_config = true;
+    else if (a == "--precision") c.precision = next_arg(i, argc, argv, a);
+    else if (a == "--rng") c.rng = next_arg(i, argc, argv, a);
+    else if (a == "--backmap-mode") c.backmap_mode = next_arg(i, argc, argv, a);
+    else if (a == "--start-policy") {
+      if (next_arg(i, argc, argv, a) != "file") die_usage("invalid --start-policy (only 'file' is supported)");
+    } else if (a == "--iter-rounding-passes" || a == "--iter-rounding-warmup" || a == "--affine-hull-tol" ||
+               a == "--pair-schedule" || a == "--pair-schedule-file" || a == "--extra-constraint-eps" ||
+               a == "--constraint-eps") {
+      die_usage("unsupported flag: " + a);
+    } else die_usage("unknown flag: " + a);
+  }
+  if (c.model_dir.empty()) die_usage("missing --model-dir");
+  if (out_root.empty()) die_usage("missing --out-root");
+  if (c.n_chains <= 0) die_usage("invalid --n-chains");
+  if (c.n_samples <= 0) die_usage("invalid --n-samples");
+  if (c.pair_prob < 0.0 || c.pair_prob > 1.0) die_usage("invalid --pair-prob (must be in [0,1])");
+  if (c.resync_interval < 0) die_usage("invalid --resync-interval (must be >=0)");
+  if (c.ksparse_prob < 0.0 || c.ksparse_prob > 1.0) die_usage("invalid --ksparse-prob (must be in [0,1])");
+  if (c.ksparse_k <= 0) die_usage("invalid --ksparse-k (must be >0)");
+  if (c.extra_constraints != "auto" && c.extra_constraints != "ignore" && c.extra_constraints != "require")
+    die_usage("invalid --extra-constraints (auto|ignore|require)");
+  if (c.bounds_policy != "ignore" && c.bounds_policy != "filter") die_usage("invalid --bounds-policy: " + c.bounds_policy);
+  if (c.precision != "fp32" && c.precision != "fp64") die_usage("invalid --precision (fp32|fp64)");
+  if (c.rng != "philox" && c.rng != "mrg") die_usage("invalid --rng (philox|mrg)");
+  if (c.backmap_mode != "fp64" && c.backmap_mode != "tf32x3" && c.backmap_mode != "bf16x3")
+    die_usage("invalid --backmap-mode (fp64|tf32x3|bf16x3)");
+  if (c.bounds_policy == "filter" && !c.backmap) throw std::runtime_error("bounds-policy=filter requires --backmap");
+
+  std::string md = c.model_dir;
+  if (!md.empty() && md.back() == '/') md.pop_back();
+  if (!is_directory(md)) throw std::runtime_error("model-dir is not a directory: " + md);
+  const auto slash = md.find_last_of('/');
+  c.model_dir = md;
+  c.model_name = slash == std::string::npos ? md : md.substr(slash + 1);
+  c.rounding_dir = md + "/rounding";
+  c.gem_dir = md + "/gem";
+  c.data_dir = slash == std::string::npos ? "." : md.substr(0, slash);
+  validate_contract(c);
+  c.out_dir = allocate_run_dir(out_root, c.model_name);
+  const bool st = !c.quiet;
+  phase(st, "validate model contract");
+  phase(st, "write generated config");
+  const std::string gen = c.out_dir + "/config_generated.txt";
+  write_generated_config(gen, c);
+  if (c.print_config) {
+    std::cout << "config_generated    :: " << absolute(gen) << "\n---\n";
+    std::ifstream f(gen);
+    std::cout << f.rdbuf() << "---\n";
+  }
+  std::vector<std::string> full = {"naja", "sample", "run"};
+  for (int i = 0; i < argc; ++i) full.push_back(argv[i]);
+  write_run_manifest(c, full);
+  kv(st, "model", c.model_name);
+  kv(st, "output", absolute(c.out_dir));
+  kv(st, "bounds", c.bounds_policy);
+  if (c.bounds_policy == "filter") kv(st, "bounds_eps", std::to_string(c.bounds_eps));
+  if (c.dry_run) {
+    phase(st, "dry-run: not executing sampling");
+    return 0;
+  }
+  phase(st, "sampling");
+  return run_sampling(c);
+}
+
+// ------------------------------------------------------------ validate
+float percentile(std::vector<float> v, float q) {
+  if (v.empty()) return 0.0f;
+  std::sort(v.begin(), v.end());
+  const float pos = q * static_cast<float>(v.size() - 1);
+  const int lo = static_cast<int>(std::floor(pos)), hi = static_cast<int>(std::ceil(pos));
+  if (lo == hi) return v[lo];
+  const float t = pos - static_cast<float>(lo);
+  return v[lo] * (1.0f - t) + v[hi] * t;
+}
+
+[[noreturn]] void die_validate(const std::string& msg) {
+  std::cerr << "error: " << msg << "\n\nusage:\n  naja validate --samples <file.npy> [--model-dir <dir>] [--n-chains 4]\n";
+  std::exit(2);
+}
+
+int cmd_validate(int argc, char** argv) {
+  std::string samples_path, model_dir;
+  int n_chains = 4, gpu = 0;
+  for (int i = 0; i < argc; ++i) {
+    const std::string a = argv[i];
+    auto nxt = [&]() -> std::string {
+      if (i + 1 >= argc) die_validate("missing value for " + a);
+      return argv[++i];
+    };
+    if (a == "--samples") samples_path = nxt();
+    else if (a == "--model-dir") model_dir = nxt();
+    else if (a == "--n-chains") n_chains = std::stoi(nxt());
+    else if (a == "--gpu") gpu = std::stoi(nxt());
+    else die_validate("unknown flag: " + a);
+  }
+  (void)gpu;
+  if (samples_path.empty()) die_validate("missing --samples");
+  if (n_chains < 1) die_validate("--n-chains must be >= 1");
+  std::cerr << "loading " << samples_path << "..." << std::endl;
+  long long rows = 0, cols = 0;
+  std::vector<float> raw = load_npy(samples_path, &rows, &cols);
+  // (n_samples, dim) rows are samples; the reference takes the smaller
+  // extent as the dimension (validate_cli.cpp:96-99)
+  const long long dim = std::min(rows, cols), n_total = std::max(rows, cols);
+  std::vector<float> S;
+  if (rows >= cols) {
+    S.swap(raw);
+  } else {
+    S.resize(raw.size());
+    for (long long dd = 0; dd < dim; ++dd)
+      for (long long s = 0; s < n_total; ++s) S[s * dim + dd] = raw[dd * n_total + s];
+  }
+  const long long spc = n_total / n_chains;
+  std::cerr << "  shape: (" << dim << ", " << n_total << ") = " << n_chains << " chains x " << spc << " samples" << std::endl;
+  if (n_total % n_chains != 0)
+    throw std::runtime_error("n_total (" + std::to_string(n_total) + ") not divisible by n_chains (" +
+                             std::to_string(n_chains) + ")");
+  int active = 0;
+  for (long long dd = 0; dd < dim; ++dd) {
+    double mean = 0, var = 0;
+    for (long long s = 0; s < n_total; ++s) mean += S[s * dim + dd];
+    mean /= n_total;
+    for (long long s = 0; s < n_total; ++s) var += (S[s * dim + dd] - mean) * (S[s * dim + dd] - mean);
+    if (var / n_total > 1e-20) ++active;
+  }
+  std::cerr << "  computing ESS..." << std::endl << "  computing split-R-hat..." << std::endl;
+  std::vector<double> ess(static_cast<size_t>(dim) * n_chains), rh(static_cast<size_t>(dim));
+  check(naja_validate(S.data(), n_total, static_cast<int>(dim), n_chains, 0, ess.data(), rh.data(), nullptr));
+  std::vector<float> ess_dim(dim), rh_f(dim);
+  for (long long dd = 0; dd < dim; ++dd) {
+    double mn = 1e300;
+    for (int k = 0; k < n_chains; ++k) mn = std::min(mn, ess[dd * n_chains + k]);
+    ess_dim[dd] = static_cast<float>(mn);
+    rh_f[dd] = static_cast<float>(rh[dd]);
+  }
+  const float ess_min = *std::min_element(ess_dim.begin(), ess_dim.end());
+  const float ess_max = *std::max_element(ess_dim.begin(), ess_dim.end());
+  const float ess_p10 = percentile(ess_dim, 0.10f), ess_med = percentile(ess_dim, 0.50f);
+  const float rh_med = percentile(rh_f, 0.50f), rh_max = *std::max_element(rh_f.begin(), rh_f.end());
+  int a11 = 0, a12 = 0;
+  for (float r : rh_f) {
+    a11 += r > 1.1f;
+    a12 += r > 1.2f;
+  }
+  bool has_bounds = false;
+  long long n_viol = 0, n_checked = 0;
+  double worst = 0.0;
+  if (!model_dir.empty()) {
+    std::string md = model_dir;
+    if (!md.empty() && md.back() == '/') md.pop_back();
+    const auto slash = md.find_last_of('/');
+    const std::string name = slash == std::string::npos ? md : md.substr(slash + 1);
+    const std::string Tp = md + "/rounding/" + name + "_rounding_T.csv", sp = md + "/rounding/" + name + "_rounding_shift.csv";
+    const std::string lp = md + "/gem/l_bounds.csv", up = md + "/gem/u_bounds.csv";
+    if (path_exists(Tp) && path_exists(lp)) {
+      std::cerr << "  checking bounds compliance..." << std::endl;
+      const Csv T = load_csv(Tp), sh = load_csv(sp), l = load_csv(lp), u = load_csv(up);
+      if (T.cols != dim) throw std::runtime_error("T has " + std::to_string(T.cols) + " columns, samples have " + std::to_string(dim));
+      // every max(1, n/1000)-th sample (src/validate/bounds_check.cpp:8-39)
+      const long long step = std::max<long long>(1, n_total / 1000);
+      // every (sample, reaction) pair counts once; violation = max(lb - v - eps, v - ub - eps) > 0
+      for (long long s = 0; s < n_total; s += step) {
+        for (int i = 0; i < T.rows; ++i) {
+          double v = sh.v[i];
+          for (long long k = 0; k < dim; ++k) v += T.v[static_cast<size_t>(i) * T.cols + k] * S[s * dim + k];
+          ++n_checked;
+          const double viol = std::max(l.v[i] - v - 1e-6, v - u.v[i] - 1e-6);
+          if (viol > 0.0) {
+            ++n_viol;
+            worst = std::max(worst, viol);
+          }
+        }
+      }
+      has_bounds = true;
+    }
+  }
+  std::string status = "OK";
+  if (a12 > dim / 4) status = "FAIL";
+  else if (a11 > dim / 4 || ess_min < 10) status = "WARN";
+  std::cerr << "\n[" << status << "] ESS min=" << std::setprecision(0) << std::fixed << ess_min << " p10=" << ess_p10
+            << " med=" << ess_med << "  R-hat med=" << std::setprecision(3) << rh_med << " max=" << rh_max
+            << " >1.1=" << a11 << " >1.2=" << a12;
+  if (has_bounds) std::cerr << "  bounds=" << n_viol << "/" << n_checked;
+  std::cerr << std::endl;
+  std::cout << "{\n  \"samples_file\": \"" << samples_path << "\",\n  \"shape\": [" << n_total << ", " << dim << "],\n"
+            << "  \"n_chains\": " << n_chains << ",\n  \"n_samples_per_chain\": " << spc << ",\n"
+            << "  \"active_dims\": " << active << ",\n  \"status\": \"" << status << "\",\n"
+            << "  \"ess\": {\n    \"min\": " << std::setprecision(1) << std::fixed << ess_min << ",\n"
+            << "    \"p10\": " << ess_p10 << ",\n    \"median\": " << ess_med << ",\n    \"max\": " << ess_max << "\n  },\n"
+            << "  \"rhat\": {\n    \"median\": " << std::setprecision(4) << rh_med << ",\n    \"max\": " << rh_max << ",\n"
+            << "    \"above_1_1\": " << a11 << ",\n    \"above_1_2\": " << a12 << "\n  }";
+  if (has_bounds)
+    std::cout << ",\n  \"bounds\": {\n    \"n_checked\": " << n_checked << ",\n    \"n_violations\": " << n_viol
+              << ",\n    \"max_violation\": " << std::setprecision(6) << worst << "\n  }";
+  std::cout << "\n}\n";
+  return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  try {
+    if (argc >= 3 && std::string(argv[1]) == "sample" && std::string(argv[2]) == "run")
+      return cmd_sample_run(argc - 3, argv + 3);
+    if (argc >= 2 && std::string(argv[1]) == "validate") return cmd_validate(argc - 2, argv + 2);
+    if (argc >= 2 && std::string(argv[1]) == "version") {
+      std::cout << naja_version() << std::endl;
+      return 0;
+    }
+    std::cerr << "usage:\n  naja sample run --model-dir <dir> --out-root <dir> --n-chains K --n-samples S [...]\n"
+              << "  naja validate --samples <file.npy> [--model-dir <dir>] [--n-chains 4]\n  naja version\n";
+    return 2;
+  } catch (const std::exception& e) {
+    std::cerr << "error: " << e.what() << std::endl;
+    return 1;
+  }
+}
