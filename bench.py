@@ -408,6 +408,78 @@ def _batched(a, torch, dev):
                                    key=lambda r: -r["M_steps_per_s"])[:5]}
 
 
+def _precision_study(a):
+    """FP32 tier with FP64 recompute every K steps against the FP64 tier, and
+    the split-precision backmap against FP64, on the genome-shaped polytope at
+    d=1500, n=7000 (m=14000): 8 chains x 200 samples, thinning 250,
+    pair-prob 0.3, identical Philox streams for every run.  Per run: kernel
+    time, polytope bound violations (A y <= b + 1e-6 max(1,|b|)), and the
+    position divergence from the FP64 run (max and RMS over all saved
+    coordinates, relative to the coordinate's range in the FP64 run).  Backmap:
+    max / RMS relative error over 20,000 samples (|v| > 1e-3 max|v|) and the
+    time of 200,000 samples per mode."""
+    import torch
+
+    from naja_b200 import Polytope, backmap, synth
+
+    g = synth.genome_shaped(n=7000, d=1500, density=0.08, seed_T=0, seed_u=1)
+    A, b = g["A"], g["b"]
+    dev = torch.device("cuda:0")
+    P = Polytope(A, b)
+    nch, nspc, thin = 8, 200, 250
+    X0 = np.zeros((nch, 1500))
+    At = torch.from_numpy(A).to(dev)
+    bt = torch.from_numpy(b).to(dev)
+    tol = 1e-6 * torch.clamp(bt.abs(), min=1.0)
+
+    def run(precision, K):
+        P.run(X0, 2, thin, nch, seed=a.seed, pair_prob=0.3, precision=precision, resync_interval=K)  # warm
+        out = torch.empty((nspc * nch, 1500), dtype=torch.float64, device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        P.run(X0, nspc, thin, nch, seed=a.seed, pair_prob=0.3, precision=precision, resync_interval=K, out=out,
+              out_dtype="f64")
+        e1.record()
+        torch.cuda.synchronize()
+        r = out @ At.T - bt
+        return out, e0.elapsed_time(e1), int((r > tol).sum()), float(r.max())
+
+    ref, t64, v64, w64 = run("fp64", 0)
+    span = (ref.max(dim=0).values - ref.min(dim=0).values).clamp(min=1e-12)
+    rows = [{"tier": "fp64", "K": 0, "ms": t64, "bound_violations": v64, "worst_violation": w64}]
+    for K in (0, 1024, 256, 64):
+        y, t, v, w = run("fp32", K)
+        rel = (y - ref).abs() / span
+        rows.append({"tier": "fp32", "K": K, "ms": t, "time_vs_fp64": t / t64, "bound_violations": v,
+                     "worst_violation": w, "divergence_max": float(rel.max()),
+                     "divergence_rms": float(rel.pow(2).mean().sqrt())})
+    T = torch.from_numpy(g["T"]).to(dev)
+    sh = torch.from_numpy(g["shift"]).to(dev)
+    Y = ref.float()
+    Ybig = Y.repeat((200000 + Y.shape[0] - 1) // Y.shape[0], 1)[:200000].contiguous()
+    bm = {}
+    ysub = Ybig[:20000]
+    vref = ysub.double() @ T.T + sh
+    nz = vref.abs() > 1e-3 * vref.abs().max()
+    for mode in ("fp64", "bf16x3", "tf32x3"):
+        V = torch.empty((20000, 7000), dtype=torch.float32, device=dev)
+        backmap(g["T"], g["shift"], ysub, mode=mode, out=V)
+        rel = ((V.double() - vref).abs()[nz] / vref.abs()[nz])
+        Vb = torch.empty((200000, 7000), dtype=torch.float32, device=dev)
+        backmap(g["T"], g["shift"], Ybig, mode=mode, out=Vb)  # warm
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        backmap(g["T"], g["shift"], Ybig, mode=mode, out=Vb)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        bm[mode] = {"max_rel": float(rel.max()), "rms_rel": float(rel.pow(2).mean().sqrt()), "ms_200k": ms,
+                    "tflops": 2.0 * 7000 * 1500 * 200000 / (ms / 1e3) / 1e12}
+        del V, Vb
+    return {"workload": "genome-shaped n=7000 d=1500 m=14000, 8 chains x 200 samples, thinning 250, pair 0.3",
+            "chr": rows, "backmap": bm}
+
+
 def _learned(a):
     """Learned vs Dikin vs plain CHR on held-out conditioned variants of the
     genome-shaped polytope (the batched-variant generator): the rounding
@@ -537,11 +609,16 @@ def main(argv=None):
                     help="learned-rounding section: training variants (0 = skip)")
     ap.add_argument("--learned-test", type=int, default=16)
     ap.add_argument("--learned-epochs", type=int, default=60)
+    ap.add_argument("--precision-study", action="store_true",
+                    help="run only the FP32/FP64 tier and backmap precision study and print it")
     a = ap.parse_args(argv)
     if a.warmup < 3:
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if a.precision_study:
+        print(json.dumps(_precision_study(a)))
+        return
     if a.impl == "reference":
         # rank 0 alone times the reference; the other ranks exit without work
         if rank == 0:

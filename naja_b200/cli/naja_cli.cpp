@@ -767,14 +767,24 @@ int cmd_validate(int argc, char** argv) {
     if (path_exists(Tp) && path_exists(lp)) {
       std::cerr << "  checking bounds compliance..." << std::endl;
       const Csv T = load_csv(Tp), sh = load_csv(sp), l = load_csv(lp), u = load_csv(up);
-      if (T.cols != dim) throw std::runtime_error("T has " + std::to_string(T.cols) + " columns, samples have " + std::to_string(dim));
+      // samples in the reduced space are mapped with v = T y + shift; samples
+      // written with --backmap are already in reaction space and checked as they are
+      const bool reduced = T.cols == dim;
+      if (!reduced && T.rows != dim)
+        throw std::runtime_error("samples have " + std::to_string(dim) + " values, T is " + std::to_string(T.rows) +
+                                 " x " + std::to_string(T.cols));
       // every max(1, n/1000)-th sample (src/validate/bounds_check.cpp:8-39)
       const long long step = std::max<long long>(1, n_total / 1000);
       // every (sample, reaction) pair counts once; violation = max(lb - v - eps, v - ub - eps) > 0
       for (long long s = 0; s < n_total; s += step) {
         for (int i = 0; i < T.rows; ++i) {
-          double v = sh.v[i];
-          for (long long k = 0; k < dim; ++k) v += T.v[static_cast<size_t>(i) * T.cols + k] * S[s * dim + k];
+          double v;
+          if (reduced) {
+            v = sh.v[i];
+            for (long long k = 0; k < dim; ++k) v += T.v[static_cast<size_t>(i) * T.cols + k] * S[s * dim + k];
+          } else {
+            v = S[s * dim + i];
+          }
           ++n_checked;
           const double viol = std::max(l.v[i] - v - 1e-6, v - u.v[i] - 1e-6);
           if (viol > 0.0) {

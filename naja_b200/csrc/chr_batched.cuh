@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(NT + 32, NT >= 512 ? 2 : (NT == 256 ? 3 : 4))
     if (threadIdx.x >= NT) {
       if (threadIdx.x == NT) producer_entry<Real>(item_args, L, smem, ch);
     } else {
-      run_consumers<Real, NT, R, kBatchV, SS, false, false>(item_args, L, smem, ch);
+      run_consumers<Real, NT, R, kBatchV, SS, false>(item_args, L, smem, ch);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
