@@ -641,6 +641,9 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
 #pragma unroll
           for (int v = 0; v < V; ++v) acc[v] = 0.0;
           const double* Ar = a.A64 + base;
+          // Unrolled so that the loads of several columns are in flight
+          // ahead of the (sequential, order-preserving) fma chain.
+#pragma unroll 4
           for (int j = 0; j < d; ++j) {
             const double xj = xs[j];
             const double* Aj = Ar + static_cast<size_t>(j) * lda;
