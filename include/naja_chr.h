@@ -78,6 +78,9 @@ typedef struct naja_chr_params {
     void* rng_state;       /* nullable MRG32k3a states (naja_mrg_state_bytes each), in/out */
     unsigned long long* wait_cycles; /* nullable device buffer, 4 per chain: consumer wait for columns,
                                         producer wait for slots, consumer loop, producer loop (SM cycles) */
+    int cluster;           /* CTAs per chain: 0 = automatic (one CTA per chain), 1 = one CTA per
+                              chain, 2..8 = a chain's rows split over a thread-block cluster of that
+                              many CTAs (128 or 256 threads each); results are identical for every value */
 } naja_chr_params;
 
 /* Fills `p` with the reference's defaults (gpusamplers.h:30-46): tpb auto,

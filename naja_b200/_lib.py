@@ -109,6 +109,7 @@ class ChrParams(C.Structure):
         ("max_slots", C.c_int),
         ("rng_state", C.c_void_p),
         ("wait_cycles", C.c_void_p),
+        ("cluster", C.c_int),
     ]
 
 

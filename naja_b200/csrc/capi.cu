@@ -71,6 +71,7 @@ const char* dev_error_name(int code) {
     case kDevTimeoutEmpty: return "the producer timed out waiting for a free slot";
     case kDevTimeoutDrain: return "the exit path timed out draining its bulk copies";
     case kDevBadPair: return "pair schedule index outside [0, d)";
+    case kDevTimeoutCluster: return "a CTA of a chain's cluster timed out waiting for its peers";
     default: return "unknown device error";
   }
 }
@@ -260,7 +261,13 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
 
   ChrLaunchConfig cfg;
-  int st = chr_plan(p->precision, P->m, P->d, P->lda, p->tpb, p->max_slots, &cfg);
+  if (p->cluster < 0 || p->cluster > 8)
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run: cluster must be 0 (automatic) or 1..8");
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
+  // carried MRG states are read and written by one CTA per chain
+  const int cluster_req = p->rng_state ? 1 : p->cluster;
+  int st = chr_plan(p->precision, P->m, P->d, P->lda, p->tpb, p->max_slots, p->nchains, cluster_req, sms, &cfg);
   if (st == NAJA_ERR_INVALID_ARGUMENT) return fail(st, "Invalid threads per block");
   if (st) return fail(st, "CoordinateHitAndRun: shape (m=" + std::to_string(P->m) + ", d=" + std::to_string(P->d) +
                               ") exceeds the step kernel's capacity for this thread count");

@@ -46,17 +46,23 @@ struct ChrArgs {
 };
 
 struct ChrLaunchConfig {
-  int threads;    // consumer threads per chain (multiple of 32)
+  int threads;    // consumer threads per CTA (multiple of 32)
   int rows;       // row chunks held per consumer warp (template capacity)
   int slots;      // staged-column ring depth (0 = read columns straight from L2/HBM)
   size_t smem;    // dynamic shared memory bytes
+  int cluster;    // CTAs per chain (thread-block cluster); 1 = one CTA per chain
+  int slice_lda;  // rows a CTA's column slot holds (cluster > 1), padded to 32
 };
 
 // Picks a launch configuration.  `tpb` > 0 forces the consumer thread count
 // (one of the reference's 32, 64, 128, 256, 512, 1024; 1024 runs as 992 consumer
 // threads plus the producer warp); `max_slots` > 0 caps the ring.
 // Returns 0 or a naja status code.
-int chr_plan(int precision, int m, int d, int lda, int tpb, int max_slots, ChrLaunchConfig* out);
+// `cluster`: CTAs per chain, 0 = automatic (one CTA per chain), 1 = one CTA
+// per chain, 2..8 = a thread-block cluster of that many CTAs per chain;
+// `nchains` and `sms` are the launch's chains and the device's SMs.
+int chr_plan(int precision, int m, int d, int lda, int tpb, int max_slots, int nchains, int cluster, int sms,
+             ChrLaunchConfig* out);
 
 // Launches nchains independent chains (one CTA each) on `stream`.
 int chr_launch(int precision, const ChrArgs& args, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);

@@ -46,7 +46,8 @@ int max_chunks_for(int threads) { return threads <= 512 ? 16 : 8; }
 
 }  // namespace
 
-int chr_plan(int precision, int m, int d, int lda, int tpb, int max_slots, ChrLaunchConfig* out) {
+namespace {
+int plan_single(int precision, int m, int d, int lda, int tpb, int max_slots, ChrLaunchConfig* out) {
   const int elt = precision == NAJA_PREC_FP64 ? 8 : 4;
   int threads = 0;
   if (tpb > 0) {
@@ -55,10 +56,13 @@ int chr_plan(int precision, int m, int d, int lda, int tpb, int max_slots, ChrLa
     if (tpb != 32 && tpb != 64 && tpb != 128 && tpb != 256 && tpb != 512 && tpb != 1024) return NAJA_ERR_INVALID_ARGUMENT;
     threads = tpb == 1024 ? 992 : tpb;
   } else {
-    // Automatic: about 8 rows per thread, at least one warp, at most 992.
+    // Automatic: at most 12 rows per thread, 992 threads only when 512 would
+    // hold more than 16.  Fewer warps per chain carry less per-step fixed
+    // work: at m = 5200 a step takes 2.07 us with 512 threads, 2.56 us with
+    // 992 and 3.26 us with 256 (B200, 16 chains).
     threads = 32;
-    while (threads < 512 && (m + threads - 1) / threads > 8) threads *= 2;
-    if ((m + threads - 1) / threads > 8) threads = 992;
+    while (threads < 512 && (m + threads - 1) / threads > 12) threads *= 2;
+    if ((m + threads - 1) / threads > 16) threads = 992;
   }
   const int chunk = 32 * kStandaloneV;
   const int chunks = (m + chunk - 1) / chunk, warps = threads / 32;
@@ -81,7 +85,62 @@ int chr_plan(int precision, int m, int d, int lda, int tpb, int max_slots, ChrLa
   out->rows = rows;
   out->slots = slots;
   out->smem = L.total;
+  out->cluster = 1;
+  out->slice_lda = lda;
   return NAJA_OK;
+}
+
+// A chain over `cs` CTAs: 128 or 256 consumer threads per CTA (about 8 rows
+// per thread of the CTA's slice), the slot ring sized for the slice.
+int plan_cluster(int precision, int m, int d, int tpb, int max_slots, int cs, ChrLaunchConfig* out) {
+  const int elt = precision == NAJA_PREC_FP64 ? 8 : 4;
+  const int chunk = 32 * kStandaloneV;
+  const int nc = (m + chunk - 1) / chunk;
+  if (cs < 2 || cs > 8 || nc < cs) return NAJA_ERR_UNSUPPORTED;
+  const int slice_chunks = (nc + cs - 1) / cs;
+  const int slice_rows = slice_chunks * chunk;
+  int threads;
+  if (tpb > 0) {
+    if (tpb != 128 && tpb != 256) return NAJA_ERR_UNSUPPORTED;
+    threads = tpb;
+  } else {
+    threads = (slice_rows + 127) / 128 > 8 ? 256 : 128;
+  }
+  const int warps = threads / 32;
+  int rows = 1;
+  while (rows * warps < slice_chunks) rows *= 2;
+  if (rows > max_chunks_for(threads)) return NAJA_ERR_UNSUPPORTED;
+  const int slda = (slice_rows + 31) / 32 * 32;
+  int slots = kMaxSlots;
+  if (max_slots > 0 && max_slots < slots) slots = max_slots;
+  Layout L = make_layout(d, slda, elt, threads, slots);
+  // the cluster kernel also holds ~1 KB of static shared memory
+  while (slots >= 3 && L.total + 1024 > kSmemBudget) {
+    --slots;
+    L = make_layout(d, slda, elt, threads, slots);
+  }
+  if (L.total + 1024 > kSmemBudget || slots < 3) return NAJA_ERR_UNSUPPORTED;
+  out->threads = threads;
+  out->rows = rows;
+  out->slots = slots;
+  out->smem = L.total;
+  out->cluster = cs;
+  out->slice_lda = slda;
+  return NAJA_OK;
+}
+}  // namespace
+
+int chr_plan(int precision, int m, int d, int lda, int tpb, int max_slots, int nchains, int cluster, int sms,
+             ChrLaunchConfig* out) {
+  if (cluster < 0 || cluster > 8) return NAJA_ERR_INVALID_ARGUMENT;
+  // Automatic is one CTA per chain: splitting a chain over a cluster was
+  // measured slower at every size tried (16 chains, m = 5200: 2.8-6.8 us per
+  // step against 2.07 us), the cross-SM exchange costing more per step than
+  // the split rows save.  The split stays available on request.
+  (void)nchains;
+  (void)sms;
+  if (cluster >= 2) return plan_cluster(precision, m, d, tpb, max_slots, cluster, out);
+  return plan_single(precision, m, d, lda, tpb, max_slots, out);
 }
 
 int chr_launch(int precision, const ChrArgs& args, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream) {

@@ -554,6 +554,20 @@ __device__ __forceinline__ void vstore(Real* p, const Real (&v)[V]) {
   }
 }
 
+// Cross-CTA exchange of a chain split over a thread-block cluster: entry
+// [buffer][rank] holds rank's (hi, lo, lo2, abort) of one step, written by
+// the owner into every peer's copy; `bar[buffer]` completes when all CTAs
+// of the cluster have written.  Buffers alternate between steps.
+struct ClusterXEntry {
+  unsigned long long hi, lo, lo2, abort;
+};
+struct ClusterCtx {
+  ClusterXEntry* xbuf;  // [2][size]
+  uint64_t* bar;        // [2], expected count = size
+  int* flag;            // [2], outcome of the local wait
+  uint32_t rank, size;
+};
+
 // Consumer side of one chain.
 //
 // Rows are handed out in chunks of C = 32 V rows: chunk c covers rows
@@ -566,8 +580,10 @@ __device__ __forceinline__ void vstore(Real* p, const Real (&v)[V]) {
 // SS: slack in shared memory (row r of this chain at slack[r]) instead of
 // the consumer threads' registers; used by the batched kernel so that several
 // chains share an SM without register pressure.
-template <class Real, int NT, int R, int V, bool SS = false, bool TIMING = true, bool MAYBE_DIRECT = true>
-__device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* smem, int chain_local) {
+template <class Real, int NT, int R, int V, bool SS = false, bool TIMING = true, bool MAYBE_DIRECT = true,
+          bool CL = false>
+__device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* smem, int chain_local,
+                              const ClusterCtx* cx = nullptr) {
   using T = Tier<Real>;
   using Acc = typename T::Acc;
   using UT = typename T::UType;
@@ -823,6 +839,42 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
     } else {
       ok = !__any_sync(0xffffffffu, !ok);
     }
+    if constexpr (CL) {
+      // The CTA's values are uniform here.  Thread 0 writes them into every
+      // CTA of the cluster, arrives on their barriers (releasing the writes)
+      // and waits, bounded, for all entries of this step; one named barrier
+      // hands the outcome to the other threads, so every warp takes the same
+      // decision.  The abort flag travels with the values: all CTAs of the
+      // chain leave at the same step.
+      const int xb = static_cast<int>(t & 1);
+      if (tid == 0) {
+        ClusterXEntry* mine = cx->xbuf + xb * cx->size + cx->rank;
+        for (uint32_t q = 0; q < cx->size; ++q) {
+          const uint32_t ra = cluster_map(mine, q);
+          cluster_st_v2(ra, static_cast<unsigned long long>(hi), static_cast<unsigned long long>(lo));
+          cluster_st_v2(ra + 16, static_cast<unsigned long long>(lo2), ok ? 0ull : 1ull);
+        }
+        for (uint32_t q = 0; q < cx->size; ++q) mbar_arrive_remote(cluster_map(&cx->bar[xb], q));
+        const bool w = mbar_wait_cluster_bounded(&cx->bar[xb], static_cast<uint32_t>((t >> 1) & 1), a.timeout_ns);
+        cx->flag[xb] = w ? 1 : 0;
+        if (!w) set_error(a.err, kDevTimeoutCluster, static_cast<int>(cx->rank), static_cast<int>(t), 0);
+      }
+      named_bar_sync(1, NT);
+      const bool arrived = cx->flag[xb] != 0;
+      Acc h = T::acc_hi0(), l = T::acc_lo0(), l2 = T::acc_lo20();
+      int bflag = arrived ? 0 : 1;
+      if (arrived && lane < static_cast<int>(cx->size)) {
+        const ClusterXEntry& e = cx->xbuf[xb * cx->size + lane];
+        h = static_cast<Acc>(e.hi);
+        l = static_cast<Acc>(e.lo);
+        l2 = static_cast<Acc>(e.lo2);
+        bflag = e.abort != 0ull;
+      }
+      hi = T::red_hi(h);
+      lo = T::red_lo(l);
+      lo2 = T::red_lo2(l2);
+      ok = !__any_sync(0xffffffffu, bflag);
+    }
     if (!ok) {
       if (tid == 0) {
         set_error(a.err, kDevTimeoutFull, sa, static_cast<int>(parity), static_cast<int>(t));
@@ -847,7 +899,7 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
         if (idx % NT == tid) xs[idx] = __fma_rn(a64, T::coef(M.ks_coef[q]), xs[idx]);
       }
     }
-    if (thin_ctr == 0) {
+    if (thin_ctr == 0 && a.samples) {
       if (a.out_f64) {
         double* out = reinterpret_cast<double*>(a.samples) + out_row * d;
         for (int j = tid; j < d; j += NT) out[j] = xs[j];
@@ -922,9 +974,93 @@ __global__ void __launch_bounds__(NT + 32, 1)
   run_consumers<Real, NT, R, kStandaloneV>(a, L, smem, chain_local);
 }
 
+// One chain split over a thread-block cluster of `size` CTAs: CTA `rank`
+// owns the row chunks [nc rank / size, nc (rank + 1) / size) of the 32 V-row
+// chunks, with its own column staging (producer), slack and FP64 recompute
+// of those rows, a full copy of x and the same direction stream, so every
+// CTA computes the same alpha from the cluster-wide extremes.  Only rank 0
+// writes samples and final positions.  The kernel begins and ends with a
+// barrier over the whole cluster: no CTA starts sending before every peer
+// has initialised its barriers, and none leaves while a peer may still write
+// into its shared memory.
+template <class Real, int NT, int R>
+__global__ void __launch_bounds__(NT + 32, 1)
+    chr_cluster_kernel(const __grid_constant__ ChrArgs base, const __grid_constant__ Layout L) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ ChrArgs slice;
+  __shared__ __align__(16) ClusterXEntry xbuf[2 * 8];
+  __shared__ __align__(8) uint64_t xbar[2];
+  __shared__ int xflag[2];
+  const uint32_t rank = cluster_rank(), size = cluster_size();
+  const int chain_local = static_cast<int>(blockIdx.x / size);
+  constexpr int C = 32 * kStandaloneV;
+  const int nc = (base.m + C - 1) / C;
+  const int c0 = static_cast<int>(static_cast<long long>(nc) * rank / size);
+  const int c1 = static_cast<int>(static_cast<long long>(nc) * (rank + 1) / size);
+  const int row0 = c0 * C;
+  if (threadIdx.x == 0) {
+    ChrArgs a = base;
+    a.A32 = base.A32 ? base.A32 + row0 : nullptr;
+    a.A64 = base.A64 + row0;
+    a.b = base.b + row0;
+    a.m = min(c1 * C, base.m) - row0;
+    if (rank != 0) {
+      a.samples = nullptr;
+      a.X_final = nullptr;
+      a.wait_cycles = nullptr;
+    }
+    slice = a;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);
+    uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
+    for (int s = 0; s < L.slots; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NT / 32);
+    }
+    mbar_init(&xbar[0], size);
+    mbar_init(&xbar[1], size);
+    xflag[0] = xflag[1] = 0;
+    *reinterpret_cast<volatile int*>(smem + L.flag_off) = 0;
+    fence_mbar_init();
+  }
+  cluster_sync_all();
+  const ClusterCtx cx{xbuf, xbar, xflag, rank, size};
+  if (threadIdx.x >= NT) {
+    if (threadIdx.x == NT) producer_entry<Real>(slice, L, smem, chain_local);
+  } else {
+    run_consumers<Real, NT, R, kStandaloneV, false, true, true, true>(slice, L, smem, chain_local, &cx);
+  }
+  cluster_sync_all();
+}
+
 // ------------------------------------------------------------- dispatch
 template <class Real, int NT, int R>
+int launch_one_cluster(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream) {
+  auto kern = chr_cluster_kernel<Real, NT, R>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(cfg.smem));
+  if (e != cudaSuccess) return NAJA_ERR_CUDA;
+  const Layout L = make_layout(a.d, cfg.slice_lda, sizeof(Real), NT, cfg.slots);
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(static_cast<unsigned>(nchains * cfg.cluster));
+  lc.blockDim = dim3(NT + 32);
+  lc.dynamicSmemBytes = cfg.smem;
+  lc.stream = stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = static_cast<unsigned>(cfg.cluster);
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  e = cudaLaunchKernelEx(&lc, kern, a, L);
+  return e == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
+}
+
+template <class Real, int NT, int R>
 int launch_one(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream) {
+  if constexpr (NT == 128 || NT == 256) {
+    if (cfg.cluster > 1) return launch_one_cluster<Real, NT, R>(a, nchains, cfg, stream);
+  }
+  if (cfg.cluster > 1) return NAJA_ERR_UNSUPPORTED;
   auto kern = chr_kernel<Real, NT, R>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(cfg.smem));
   if (e != cudaSuccess) return NAJA_ERR_CUDA;

@@ -105,7 +105,7 @@ class Polytope:
     def params(self, nspc, thinning, nchains, *, tpb=-1, seed=0, pair_prob=0.0, resync_interval=0,
                ksparse_prob=0.0, ksparse_k=8, pair_mode=1, pairs=None, precision="fp32", rng="philox",
                out_dtype="f32", chain_base=0, out_nchains=0, step_offset=0, max_slots=0, rng_state=None,
-               wait_cycles=None):
+               wait_cycles=None, cluster=0):
         p = ChrParams()
         load().naja_chr_params_default(C.byref(p))
         p.nspc, p.thinning, p.nchains, p.tpb = int(nspc), int(thinning), int(nchains), int(tpb)
@@ -133,6 +133,7 @@ class Polytope:
             p.rng_state = _ptr(rng_state).value
         if wait_cycles is not None:
             p.wait_cycles = _ptr(wait_cycles).value
+        p.cluster = int(cluster)
         return p, keep
 
     def run(self, X0, nspc, thinning, nchains=None, *, out=None, X_final=None, stream=None, **kw):

@@ -152,3 +152,45 @@ def test_bad_pair_index_reports_device_error(cuda):
     # the context stays usable
     out = P.run(x0, 10, 1, 2)
     assert np.isfinite(out).all()
+
+
+@pytest.mark.parametrize("cluster", [2, 3, 4, 8])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_cluster_split_bit_exact(cuda, cluster, precision):
+    """A chain's rows split over a thread-block cluster give the oracle's samples."""
+    got, ref = _run_both("genome260x70", precision, pair_prob=0.3, resync=37 if precision == "fp32" else 0,
+                         nspc=60, thin=7, nchains=3, cluster=cluster)
+    assert np.array_equal(got, ref), np.abs(got - ref).max()
+
+
+def test_cluster_split_large_model(cuda):
+    """A genome-shaped model with few chains: one CTA per chain, the automatic
+    choice and an 8-CTA cluster per chain agree, in both tiers and with
+    k-sparse moves."""
+    g = synth.genome_shaped(n=1300, d=300, density=0.08, seed_T=5, seed_u=6)
+    P = Polytope(g["A"], g["b"])
+    for precision in ("fp32", "fp64"):
+        kw = dict(seed=4, pair_prob=0.3, ksparse_prob=0.05, ksparse_k=4, resync_interval=100,
+                  precision=precision, out_dtype="f64")
+        one = P.run(g["start"], 30, 11, 4, cluster=1, **kw)
+        auto = P.run(g["start"], 30, 11, 4, cluster=0, **kw)
+        eight = P.run(g["start"], 30, 11, 4, cluster=8, **kw)
+        assert np.array_equal(one, auto) and np.array_equal(one, eight)
+
+
+def test_cluster_mrg_matches_reference_tape(cuda):
+    A, b, x0 = CASES["genome260x70"]
+    nspc, thin, nchains, seed = 30, 4, 3, 2024
+    P = Polytope(A, b)
+    got = P.run(x0, nspc, thin, nchains, seed=seed, pair_prob=0.3, precision="fp64", rng="mrg", out_dtype="f64",
+                cluster=4)
+    tape = mrg_tape(seed, nchains, 4 * nspc * thin + 8)
+    ref = O.chr_run(A, b, x0, nspc, thin, nchains, pair_prob=0.3, precision="fp64", tape=tape)
+    assert np.array_equal(got, ref)
+
+
+def test_cluster_rejects_bad_size(cuda):
+    A, b, x0 = CASES["cube8"]
+    P = Polytope(A, b)
+    with pytest.raises(InvalidArgument, match="cluster"):
+        P.run(x0, 10, 1, 2, cluster=9)
