@@ -14,10 +14,13 @@
 //                        128-byte swizzle of A_hi, A_lo, B_hi, B_lo for one
 //                        128-byte K slice into a 2-stage shared-memory ring.
 //   warp 5, one thread : MMA issuer.  Per stage 4 K-steps x 3 tcgen05.mma
-//                        into a 128 x 256 FP32 accumulator in TMEM; the
+//                        into one of two 128 x 256 FP32 accumulators in TMEM
+//                        (512 columns; tiles alternate), so a tile's MMAs run
+//                        while the epilogue drains the previous tile; the
 //                        stage is released with tcgen05.commit.
-//   warps 0-3          : epilogue.  tcgen05.ld of their 32 TMEM lanes, + shift,
-//                        stores of the tile rows to V.
+//   warps 0-3          : epilogue.  tcgen05.ld of their 32 TMEM lanes, 32 x 32
+//                        blocks transposed through shared memory, + shift,
+//                        stores of 32 consecutive values of a row each.
 // Every wait is bounded (global timer); on expiry the CTA records an error,
 // stops issuing, drains its own copies / MMAs and frees TMEM before exiting.
 #include <cuda.h>
@@ -41,7 +44,7 @@ constexpr int kTileN = 256;
 constexpr int kSliceBytes = 128;  // K extent of one stage, in bytes per row
 constexpr int kStages = 2;
 constexpr int kThreads = 192;     // warps 0-3 epilogue, 4 producer, 5 MMA
-constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kTmemCols = 512;  // two 256-column accumulators
 constexpr uint64_t kTimeoutNs = 5ull * 1000 * 1000 * 1000;
 
 constexpr uint32_t kATileBytes = kTileM * kSliceBytes;  // 16 KB
@@ -129,11 +132,13 @@ __global__ void __launch_bounds__(kThreads, 1)
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* acc_full = empty + kStages;
-  uint64_t* acc_empty = acc_full + 1;
-  uint64_t* drain_bar = acc_empty + 1;
+  uint64_t* acc_full = empty + kStages;  // [2]
+  uint64_t* acc_empty = acc_full + 2;    // [2]
+  uint64_t* drain_bar = acc_empty + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain_bar + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  // epilogue staging: one 32 x 33 float block per epilogue warp
+  float* stage_out = reinterpret_cast<float*>(smem + kStages * kStageBytes + 256);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -141,8 +146,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(acc_full, 1);
-    mbar_init(acc_empty, 4);
+    mbar_init(&acc_full[0], 1);
+    mbar_init(&acc_full[1], 1);
+    mbar_init(&acc_empty[0], 4);
+    mbar_init(&acc_empty[1], 4);
     mbar_init(drain_bar, 1);
     *abort_flag = 0;
     fence_mbar_init();
@@ -203,11 +210,13 @@ __global__ void __launch_bounds__(kThreads, 1)
       constexpr int ksteps = 4;             // 4 MMAs of 32 bytes of K per 128-byte slice
       int stage = 0;
       uint32_t parity = 0;
-      uint32_t acc_round = 0;
+      uint32_t acc_round = 0;  // tiles issued by this CTA; accumulator acc_round & 1
       bool issued = false;
       for (long long tile = blockIdx.x; tile < a.tiles && !*abort_flag; tile += gridDim.x) {
-        // the epilogue of the previous tile has read the accumulator
-        if (acc_round >= 1 && !mbar_wait_bounded(acc_empty, (acc_round - 1) & 1u, kTimeoutNs)) {
+        const uint32_t buf = acc_round & 1u, use = acc_round >> 1;
+        const uint32_t tacc = tmem + buf * static_cast<uint32_t>(kTileN);
+        // the epilogue has read this accumulator's previous tile (two tiles back)
+        if (use >= 1 && !mbar_wait_bounded(&acc_empty[buf], (use - 1) & 1u, kTimeoutNs)) {
           set_error(a.err, kTcTimeoutEpi, static_cast<int>(blockIdx.x), static_cast<int>(acc_round), -1);
           *abort_flag = 1;
           break;
@@ -232,9 +241,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint64_t ah = umma_desc_sw128(Ahi + kk * 32), al = umma_desc_sw128(Alo + kk * 32);
             const uint64_t bh = umma_desc_sw128(Bhi + kk * 32), bl = umma_desc_sw128(Blo + kk * 32);
             const uint32_t acc = (ks > 0 || kk > 0) ? 1u : 0u;
-            umma<TF32>(tmem, ah, bh, idesc, acc);
-            umma<TF32>(tmem, ah, bl, idesc, 1u);
-            umma<TF32>(tmem, al, bh, idesc, 1u);
+            umma<TF32>(tacc, ah, bh, idesc, acc);
+            umma<TF32>(tacc, ah, bl, idesc, 1u);
+            umma<TF32>(tacc, al, bh, idesc, 1u);
           }
           issued = true;
           umma_commit(&empty[stage]);  // the stage is free once these MMAs have read it
@@ -244,7 +253,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
         }
         if (!ok) break;
-        umma_commit(acc_full);  // accumulator complete
+        umma_commit(&acc_full[buf]);  // accumulator complete
         ++acc_round;
       }
       if (issued) {
@@ -255,9 +264,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else {
     // ---------------- epilogue, warps 0-3: TMEM lanes 32*warp .. 32*warp+31
+    // Each 32 x 32 block goes through shared memory so that every store
+    // instruction writes 32 consecutive values of one output row.  The
+    // other accumulator takes the next tile's MMAs meanwhile.
+    float* stg = stage_out + warp * (32 * 33);
     uint32_t acc_round = 0;
     for (long long tile = blockIdx.x; tile < a.tiles; tile += gridDim.x) {
-      bool ok = mbar_wait_bounded(acc_full, acc_round & 1u, kTimeoutNs);
+      const uint32_t buf = acc_round & 1u, use = acc_round >> 1;
+      bool ok = mbar_wait_bounded(&acc_full[buf], use & 1u, kTimeoutNs);
       if (!__all_sync(0xffffffffu, ok)) {
         if (lane == 0) set_error(a.err, kTcTimeoutAcc, static_cast<int>(blockIdx.x), warp, static_cast<int>(acc_round));
         *abort_flag = 1;
@@ -265,33 +279,41 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       tc_fence_after();
       const int tm = static_cast<int>(tile / a.tiles_n), tn = static_cast<int>(tile % a.tiles_n);
-      const long long row = static_cast<long long>(tm) * kTileM + warp * 32 + lane;
+      const long long row_base = static_cast<long long>(tm) * kTileM + warp * 32;
       const int col0 = tn * kTileN;
 #pragma unroll 1
       for (int c = 0; c < kTileN; c += 32) {
         uint32_t r[32];
-        tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c), r);
-        if (row < a.N) {
-          if (a.v_f64) {
-            double* out = reinterpret_cast<double*>(a.V) + row * a.n;
+        tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + buf * static_cast<uint32_t>(kTileN) +
+                      static_cast<uint32_t>(c),
+                  r);
 #pragma unroll
-            for (int q = 0; q < 32; ++q) {
-              const int i = col0 + c + q;
-              if (i < a.n) out[i] = static_cast<double>(__uint_as_float(r[q])) + a.shift[i];
-            }
-          } else {
-            float* out = reinterpret_cast<float*>(a.V) + row * a.n;
-#pragma unroll
-            for (int q = 0; q < 32; ++q) {
-              const int i = col0 + c + q;
-              if (i < a.n) out[i] = static_cast<float>(static_cast<double>(__uint_as_float(r[q])) + a.shift[i]);
-            }
+        for (int q = 0; q < 32; ++q) stg[lane * 33 + q] = __uint_as_float(r[q]);
+        __syncwarp();
+        const int i = col0 + c + lane;
+        const bool col_ok = i < a.n;
+        const double sh = col_ok ? a.shift[i] : 0.0;
+        if (a.v_f64) {
+#pragma unroll 4
+          for (int j = 0; j < 32; ++j) {
+            const long long row = row_base + j;
+            if (row < a.N && col_ok)
+              reinterpret_cast<double*>(a.V)[row * a.n + i] = static_cast<double>(stg[j * 33 + lane]) + sh;
+          }
+        } else {
+#pragma unroll 4
+          for (int j = 0; j < 32; ++j) {
+            const long long row = row_base + j;
+            if (row < a.N && col_ok)
+              reinterpret_cast<float*>(a.V)[row * a.n + i] =
+                  static_cast<float>(static_cast<double>(stg[j * 33 + lane]) + sh);
           }
         }
+        __syncwarp();
       }
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(acc_empty);
+      if (lane == 0) mbar_arrive(&acc_empty[buf]);
       ++acc_round;
     }
   }
@@ -424,7 +446,7 @@ int backmap_tc(int n, int d, long long N, const double* T, int ldt, const double
   a.V = V;
   a.v_f64 = v_dtype == NAJA_DTYPE_F64;
   a.err = static_cast<int*>(berr.ptr);
-  const size_t smem = kStages * kStageBytes + 1024 + 256;
+  const size_t smem = kStages * kStageBytes + 1024 + 256 + 4 * 32 * 33 * sizeof(float);
   int sms = 148;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -540,7 +562,7 @@ int backmap_tc_noalloc(int n, int d, long long N, const double* T, int ldt, cons
   a.V = V;
   a.v_f64 = v_dtype == NAJA_DTYPE_F64;
   a.err = err;
-  const size_t smem = kStages * kStageBytes + 1024 + 256;
+  const size_t smem = kStages * kStageBytes + 1024 + 256 + 4 * 32 * 33 * sizeof(float);
   int sms = 148, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

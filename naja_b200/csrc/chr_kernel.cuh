@@ -413,7 +413,7 @@ __device__ __noinline__ void run_producer(const ChrArgs& a, Src& src, const Layo
       ++round;
     }
     const unsigned long long w0 = a.wait_cycles ? clock64() : 0ull;
-    if (ra >= 1 && !mbar_wait_bounded(&empty[sa], (ra - 1) & 1u, a.timeout_ns)) {
+    if (ra >= 1 && !mbar_wait_bounded_sleep(&empty[sa], (ra - 1) & 1u, a.timeout_ns, 64)) {
       set_error(a.err, kDevTimeoutEmpty, sa, static_cast<int>(ra), static_cast<int>(t));
       *abort_flag = 1;
       break;
@@ -428,7 +428,7 @@ __device__ __noinline__ void run_producer(const ChrArgs& a, Src& src, const Layo
         slot = 0;
         ++round;
       }
-      if (rb >= 1 && !mbar_wait_bounded(&empty[sb], (rb - 1) & 1u, a.timeout_ns)) {
+      if (rb >= 1 && !mbar_wait_bounded_sleep(&empty[sb], (rb - 1) & 1u, a.timeout_ns, 64)) {
         set_error(a.err, kDevTimeoutEmpty, sb, static_cast<int>(rb), static_cast<int>(t));
         *abort_flag = 1;
         break;

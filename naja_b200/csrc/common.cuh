@@ -84,6 +84,20 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   }
 }
 
+// As mbar_wait_bounded for a thread that is not on the critical path (the
+// producer waiting for a free slot): between polls it sleeps `sleep_ns`, so
+// its polling does not take issue slots from the warps doing the work.
+__device__ __forceinline__ bool mbar_wait_bounded_sleep(uint64_t* bar, uint32_t parity, uint64_t timeout_ns,
+                                                        uint32_t sleep_ns) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 1;; ++it) {
+    __nanosleep(sleep_ns);
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 63u) == 0 && global_ns() - t0 > timeout_ns) return false;
+  }
+}
+
 // 1-D bulk copy global -> this CTA's shared memory, completing on `bar`.
 // Both addresses 16-byte aligned, size a multiple of 16 bytes.
 __device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem, uint32_t bytes, uint64_t* bar) {
