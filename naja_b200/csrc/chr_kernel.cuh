@@ -580,8 +580,12 @@ struct ClusterCtx {
 // SS: slack in shared memory (row r of this chain at slack[r]) instead of
 // the consumer threads' registers; used by the batched kernel so that several
 // chains share an SM without register pressure.
+// FUSED: the slack update of step t-1 runs inside the ratio pass of step t,
+// with step t-1's column values kept in registers (R V per lane), so each
+// step makes one pass over its rows and releases its column slot right
+// after that pass.  The values are exactly those of the two-pass order.
 template <class Real, int NT, int R, int V, bool SS = false, bool TIMING = true, bool MAYBE_DIRECT = true,
-          bool CL = false>
+          bool CL = false, bool FUSED = false>
 __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* smem, int chain_local,
                               const ClusterCtx* cx = nullptr) {
   using T = Tier<Real>;
@@ -695,6 +699,10 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
   size_t out_row = static_cast<size_t>(gchain);
   unsigned long long w_full = 0;
   const unsigned long long c_start = TIMING ? clock64() : 0ull;
+  Real ae_prev[FUSED ? R * V : 1];   // step t-1's column values of this lane's rows
+  Real ae_prev_tail[FUSED ? V : 1];  // ... of its rows in the partial chunk
+  bool pending = false;              // step t-1's slack update not applied yet
+  Real alpha_prev = Real(0);
   for (long long t = 0; t < total; ++t) {
     const int sa = slot;
     const unsigned long long w0 = (TIMING && a.wait_cycles) ? clock64() : 0ull;
@@ -743,6 +751,7 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
       if (resync_ctr == 0) {
         named_bar_sync(2, NT);  // every owner's x update of the previous step is visible
         recompute();
+        pending = false;        // the recompute already holds step t-1's move
       }
       if (++resync_ctr == a.resync) resync_ctr = 0;
     }
@@ -798,6 +807,15 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
               Real ae[V], s[V];
               vec(base, ae);
               slack_get(k, base, s);
+              if constexpr (FUSED) {
+                if (pending) {
+#pragma unroll
+                  for (int v = 0; v < V; ++v) s[v] = T::slack_update(s[v], alpha_prev, ae_prev[k * V + v]);
+                  slack_put(k, base, s);
+                }
+#pragma unroll
+                for (int v = 0; v < V; ++v) ae_prev[k * V + v] = ae[v];
+              }
 #pragma unroll
               for (int v = 0; v < V; ++v) T::acc(hi, lo, lo2, T::ratio(ae[v], s[v]));
             },
@@ -805,10 +823,28 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
 #pragma unroll
               for (int v = 0; v < V; ++v) {
                 const int r = base + v;
-                if (r < m) T::acc(hi, lo, lo2, T::ratio(one(r), slack_tail(r)));
+                if (r < m) {
+                  const Real ae = one(r);
+                  if constexpr (FUSED) {
+                    if (pending) slack_tail(r) = T::slack_update(slack_tail(r), alpha_prev, ae_prev_tail[v]);
+                    ae_prev_tail[v] = ae;
+                  }
+                  T::acc(hi, lo, lo2, T::ratio(ae, slack_tail(r)));
+                }
               }
             });
       });
+    }
+    if constexpr (FUSED) {
+      // The column is in registers now; a k-sparse step's record is still
+      // read by its x update, so that slot is released at the end.
+      if (ok && kind != kKSparse) {
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&empty[sa]);
+          if (kind == kPair) mbar_arrive(&empty[sb]);
+        }
+      }
     }
     hi = T::red_hi(hi);
     lo = T::red_lo(lo);
@@ -910,6 +946,15 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
       out_row += static_cast<size_t>(a.out_nchains);
     }
     if (++thin_ctr == a.thinning) thin_ctr = 0;
+    if constexpr (FUSED) {
+      alpha_prev = alpha;
+      pending = true;
+      if (kind == kKSparse) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[sa]);
+      }
+      continue;
+    }
     for_kind([&](auto&& vec, auto&& one) {
       for_chunks(
           [&](int k, int base) {
@@ -971,7 +1016,10 @@ __global__ void __launch_bounds__(NT + 32, 1)
     if (threadIdx.x == NT) producer_entry<Real>(a, L, smem, chain_local);
     return;
   }
-  run_consumers<Real, NT, R, kStandaloneV>(a, L, smem, chain_local);
+  // fused update where step t-1's column values (R V per lane) fit in 64
+  // bytes of registers; larger capacities keep the two-pass order
+  constexpr bool kFuse = R * kStandaloneV * sizeof(Real) <= 64;
+  run_consumers<Real, NT, R, kStandaloneV, false, true, true, false, kFuse>(a, L, smem, chain_local);
 }
 
 // One chain split over a thread-block cluster of `size` CTAs: CTA `rank`
