@@ -219,6 +219,27 @@ def _cpu_baseline(W, a, min_ess_per_step):
                       f"CPU CHR steps/s (identical trajectory)"}
 
 
+def replica_seed(seed: int, rank: int) -> int:
+    """Philox key of rank `rank`'s replica: every rank samples the same
+    workload from its own streams into its own buffers (weak scaling)."""
+    return (int(seed) + 0x9E3779B97F4A7C15 * int(rank)) & 0xFFFFFFFFFFFFFFFF
+
+
+def reduce_over_ranks(per_dim_ess, total_ms: float, world: int, device):
+    """Whole-job figures over the replicas: per-dimension ESS summed over every
+    rank's chains, device time the maximum over ranks."""
+    import torch
+
+    per_dim = np.asarray(per_dim_ess, dtype=np.float64)
+    if world <= 1:
+        return per_dim, float(total_ms)
+    t = torch.from_numpy(per_dim.copy()).to(device)
+    torch.distributed.all_reduce(t)
+    m = torch.tensor([float(total_ms)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(m, op=torch.distributed.ReduceOp.MAX)
+    return t.cpu().numpy(), float(m.item())
+
+
 def _ours(a, rank, world):
     import torch
 
@@ -235,12 +256,11 @@ def _ours(a, rank, world):
     samples = torch.empty((W.nspc * W.nchains, W.d), dtype=torch.float32, device=dev)
     V = torch.empty((W.nspc * W.nchains, W.n), dtype=torch.float32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    chain_base = rank * W.nchains
+    seed = replica_seed(a.seed, rank)
 
     def job():
-        P.run(x0, W.nspc, W.thin, W.nchains, out=samples, seed=a.seed, pair_prob=W.pair,
-              resync_interval=a.resync, precision=a.precision, chain_base=chain_base,
-              out_nchains=chain_base + W.nchains)
+        P.run(x0, W.nspc, W.thin, W.nchains, out=samples, seed=seed, pair_prob=W.pair,
+              resync_interval=a.resync, precision=a.precision)
         e_mid = torch.cuda.Event(enable_timing=True)
         e_mid.record()
         nb.backmap(T_dev, sh_dev, samples, mode=a.backmap_mode, out=V)
@@ -269,20 +289,12 @@ def _ours(a, rank, world):
         torch.cuda.synchronize()
     P.check()
     total_ms = g0.elapsed_time(g1)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
     job_ms = [ev[k][0].elapsed_time(ev[k][1]) for k in range(a.steps)]
     chr_ms = [ev[k][0].elapsed_time(mids[k]) for k in range(a.steps)]
     bm_ms = [mids[k].elapsed_time(ev[k][1]) for k in range(a.steps)]
     # metric on the last job's samples
     ess, rhat = nv.ess_rhat(samples, W.nchains, layout=1)
-    per_dim = ess.sum(axis=1)
-    if world > 1:
-        t = torch.from_numpy(per_dim).to(dev)
-        torch.distributed.all_reduce(t)
-        per_dim = t.cpu().numpy()
+    per_dim, total_ms = reduce_over_ranks(ess.sum(axis=1), total_ms, world, dev)
     min_ess = float(per_dim.min())
     ms_per_step = total_ms / a.steps
     value = min_ess / (ms_per_step / 1e3)  # min-ESS already sums every rank's chains
