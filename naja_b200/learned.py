@@ -332,7 +332,7 @@ def _diagnose(ys, nchains):
 
 def run_experiment(*, n=2600, d=700, n_train=256, n_test=16, nchains=8, nspc_train=500, nspc_test=1000,
                    thinning=116, pair_prob=0.3, rank=32, hidden=(512, 512), epochs=60, batch=64, lr=1e-3,
-                   resync=2048, seed=0, log=None):
+                   resync=2048, seed=0, train_chains=None, log=None):
     """Plain vs Dikin-rounded vs learned-rounded CHR on held-out conditioned
     variants of the genome-shaped polytope.  Returns a dict of results."""
     import time
@@ -353,7 +353,8 @@ def run_experiment(*, n=2600, d=700, n_train=256, n_test=16, nchains=8, nspc_tra
     # 1. plain CHR on the training variants -> covariance factor targets
     t0 = time.perf_counter()
     polys = [Polytope(A_list[k], b_list[k]) for k in range(n_train)]
-    ys, t_train_samp = _sample(polys, [None] * n_train, [None] * n_train, nchains, nspc_train, thinning, kw, torch)
+    ys, t_train_samp = _sample(polys, [None] * n_train, [None] * n_train, train_chains or nchains, nspc_train,
+                               thinning, kw, torch)
     T = factor_targets(torch.stack(ys), rank, torch)
     del ys, polys
     mu, sd = T.mean(axis=0), T.std(axis=0) + 1e-6
