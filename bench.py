@@ -127,13 +127,17 @@ class Workload:
         self.nchains, self.nspc, self.thin, self.pair = a.nchains, a.nspc, a.thinning, a.pair_prob
         self.steps = self.nchains * self.nspc * self.thin
         self.bytes_per_step = 4.0 * self.m * (1.0 + self.pair) + 4.0 * self.d / self.thin
+        # what the compressed-column kernel reads per step: a column's (value, row) entries, padded to pairs
+        nz = (self.A.astype(np.float32) != 0).sum(axis=0)
+        entries = np.maximum(2, nz + (nz & 1)).mean()
+        self.compressed_bytes_per_step = 8.0 * entries * (1.0 + self.pair) + 4.0 * self.d / self.thin
 
     def config(self, a):
         return {"workload": f"genome-shaped polytope n={self.n} d={self.d} m={self.m}, {self.nchains} chains x "
                             f"{self.nspc} samples, thinning {self.thin}, pair-prob {self.pair}, backmap to n={self.n}",
                 "n": self.n, "d": self.d, "m": self.m, "chains": self.nchains, "samples_per_chain": self.nspc,
                 "thinning": self.thin, "pair_prob": self.pair, "precision": a.precision,
-                "resync_interval": a.resync, "backmap": a.backmap_mode, "rng": "philox",
+                "resync_interval": a.resync, "backmap": a.backmap_mode, "rng": "philox", "step_kernel": a.sparse,
                 "l2": "256 MiB buffer written between timed steps"}
 
 
@@ -260,7 +264,7 @@ def _ours(a, rank, world):
 
     def job():
         P.run(x0, W.nspc, W.thin, W.nchains, out=samples, seed=seed, pair_prob=W.pair,
-              resync_interval=a.resync, precision=a.precision)
+              resync_interval=a.resync, precision=a.precision, sparse=a.sparse, tpb=a.tpb)
         e_mid = torch.cuda.Event(enable_timing=True)
         e_mid.record()
         nb.backmap(T_dev, sh_dev, samples, mode=a.backmap_mode, out=V)
@@ -302,6 +306,8 @@ def _ours(a, rank, world):
     bm_err = _backmap_error(torch, W, samples, V, a.backmap_mode)
     ref_sem = nv.summary(*nv.ess_rhat(samples, W.nchains, layout=0))
     peak, peak_kind = _peaks()
+    choice = P.kernel_choice(W.nspc, W.thin, W.nchains, pair_prob=W.pair, resync_interval=a.resync,
+                             precision=a.precision, sparse=a.sparse, tpb=a.tpb)
     chr_mean = statistics.mean(chr_ms)
     achieved = W.bytes_per_step * W.steps / (chr_mean / 1e3) / 1e9
     steps_per_s = W.steps * world / (ms_per_step / 1e3)
@@ -311,8 +317,14 @@ def _ours(a, rank, world):
         "dtype": "f32" if a.precision == "fp32" else "f64", "data": "synthetic (seeded genome-shaped generator)",
         "config": W.config(a),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_source": peak_kind, "kernel": "chr_kernel",
-                     "kernel_ms": chr_mean, "bytes_per_chr_step": W.bytes_per_step, "chr_steps_per_launch": W.steps},
+                     "traffic": None, "peak_source": peak_kind,
+                     "kernel": "chr_sparse_kernel" if choice["kernel"] == "columns" else "chr_kernel",
+                     "kernel_threads": choice["threads"], "kernel_ms": chr_mean,
+                     "bytes_per_chr_step": W.bytes_per_step,
+                     "bytes_definition": "4 m (1 + p_pair) + 4 d / thinning: one FP32 column per coordinate step, "
+                                         "two per pair step, plus the amortised sample write",
+                     "compressed_bytes_per_chr_step": W.compressed_bytes_per_step,
+                     "chr_steps_per_launch": W.steps},
         "chr_steps_per_s": steps_per_s, "min_ess": min_ess, "job_ms": job_ms, "chr_ms": chr_ms,
         "gate": gate,
         "backmap": {"mode": a.backmap_mode, "ms": statistics.mean(bm_ms), "error_vs_fp64": bm_err,
@@ -349,7 +361,7 @@ def _e2e(a, W, torch, dev, min_ess):
         e0.record()
         P = nb.Polytope(W.A, W.b, device=dev.index)
         P.run(x0, W.nspc, W.thin, W.nchains, out=samples, seed=a.seed, pair_prob=W.pair,
-              resync_interval=a.resync, precision=a.precision, stream=None)
+              resync_interval=a.resync, precision=a.precision, sparse=a.sparse, tpb=a.tpb, stream=None)
         nb.backmap(W.T, W.shift, samples, mode=a.backmap_mode, out=pinned_out)
         e1.record()
         torch.cuda.synchronize()
@@ -605,6 +617,9 @@ def main(argv=None):
     ap.add_argument("--pair-prob", type=float, default=0.3)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--resync", type=int, default=2048)
+    ap.add_argument("--tpb", type=int, default=-1, help="consumer threads per chain (-1 = automatic)")
+    ap.add_argument("--sparse", default="auto", choices=["auto", "dense", "columns"],
+                    help="step kernel: compressed columns, dense, or the library's automatic choice")
     ap.add_argument("--backmap-mode", default="tf32x3", choices=["fp64", "bf16x3", "tf32x3"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)

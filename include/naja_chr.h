@@ -44,6 +44,10 @@ extern "C" {
 #define NAJA_DTYPE_F32 0
 #define NAJA_DTYPE_F64 1
 
+#define NAJA_SPARSE_AUTO 0    /* compressed columns when A is at most 1/4 nonzero and they fit */
+#define NAJA_SPARSE_DENSE 1   /* every row of A every step                                     */
+#define NAJA_SPARSE_COLUMNS 2 /* only the nonzero rows of the step's column(s)                 */
+
 #define NAJA_BACKMAP_FP64 0    /* FP64 SIMT GEMM (reference arithmetic)          */
 #define NAJA_BACKMAP_BF16X3 1  /* split-BF16 on tcgen05, FP32 accumulate          */
 #define NAJA_BACKMAP_TF32X3 2  /* 3xTF32 on tcgen05, FP32 accumulate              */
@@ -81,6 +85,10 @@ typedef struct naja_chr_params {
     int cluster;           /* CTAs per chain: 0 = automatic (one CTA per chain), 1 = one CTA per
                               chain, 2..8 = a chain's rows split over a thread-block cluster of that
                               many CTAs (128 or 256 threads each); results are identical for every value */
+    int sparse;            /* NAJA_SPARSE_*: which step kernel walks A.  The compressed-column kernel
+                              takes ksparse_prob = 0 and cluster <= 1, and tpb 0 (automatic), 32, 64,
+                              128, 256 or 512 when forced (automatic selection needs tpb 0); results
+                              are identical for every value */
 } naja_chr_params;
 
 /* Fills `p` with the reference's defaults (gpusamplers.h:30-46): tpb auto,
@@ -116,6 +124,17 @@ int naja_polytope_check(const naja_polytope* P);
  * launchChrKernel (src/gpu/chr.cu:498-553). */
 int naja_chr_run(const naja_polytope* P, const naja_chr_params* params, const double* X0, int ldx,
                  void* samples, double* X_final, void* stream);
+
+/* The step kernel naja_chr_run would launch for these parameters:
+ * *sparse_kernel = 1 for the compressed-column kernel (only the nonzero rows
+ * of each step's column), 0 for the dense one; its consumer threads per
+ * chain, staged-column slots and dynamic shared memory.  Any output pointer
+ * may be null.  The first call for a polytope that may take the compressed
+ * columns builds them (device memory held until naja_polytope_destroy).  No
+ * counterpart in the reference (its launchChrKernel, src/gpu/chr.cu:498-553,
+ * has one kernel). */
+int naja_chr_kernel_choice(const naja_polytope* P, const naja_chr_params* params, int* sparse_kernel,
+                           int* threads, int* slots, size_t* smem);
 
 /* ------------------------------------------------------------- batches */
 

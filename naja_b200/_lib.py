@@ -25,6 +25,9 @@ RNG_PHILOX = 0
 RNG_REF_MRG = 1
 DTYPE_F32 = 0
 DTYPE_F64 = 1
+SPARSE_AUTO = 0     # compressed columns when A is at most 1/4 nonzero and they fit
+SPARSE_DENSE = 1    # every row of A every step
+SPARSE_COLUMNS = 2  # only the nonzero rows of the step's column(s)
 BACKMAP_FP64 = 0
 BACKMAP_BF16X3 = 1
 BACKMAP_TF32X3 = 2
@@ -37,6 +40,7 @@ EXPORTED = (
     "naja_polytope_shape",
     "naja_polytope_check",
     "naja_chr_run",
+    "naja_chr_kernel_choice",
     "naja_backmap",
     "naja_backmap_noalloc",
     "naja_validate",
@@ -110,6 +114,7 @@ class ChrParams(C.Structure):
         ("rng_state", C.c_void_p),
         ("wait_cycles", C.c_void_p),
         ("cluster", C.c_int),
+        ("sparse", C.c_int),
     ]
 
 
@@ -152,6 +157,9 @@ def load() -> C.CDLL:
     lib.naja_polytope_shape.argtypes = [vp, C.POINTER(i), C.POINTER(i)]
     lib.naja_polytope_check.argtypes = [vp]
     lib.naja_chr_run.argtypes = [vp, C.POINTER(ChrParams), vp, i, vp, vp, vp]
+    lib.naja_chr_kernel_choice.argtypes = [vp, C.POINTER(ChrParams), C.POINTER(i), C.POINTER(i), C.POINTER(i),
+                                           C.POINTER(C.c_size_t)]
+    lib.naja_chr_kernel_choice.restype = i
     lib.naja_backmap.argtypes = [i, i, ll, vp, i, vp, vp, i, vp, i, i, vp]
     lib.naja_backmap_noalloc.argtypes = [i, i, ll, vp, i, vp, vp, i, vp, i, i, vp]
     lib.naja_validate.argtypes = [vp, ll, i, i, i, vp, vp, vp]

@@ -38,6 +38,7 @@ def _units():
                           ["-fmad=false", f"-DNAJA_CHR_REAL={real}", f"-DNAJA_CHR_NT={nt}"]))
     for nt in (128, 256, 512):
         units.append((f"chr_batched_{nt}", CSRC / "chr_batched_inst.cu", ["-fmad=false", f"-DNAJA_CHR_NT={nt}"]))
+    units.append(("chr_sparse", CSRC / "chr_sparse_inst.cu", ["-fmad=false"]))
     units.append(("chr_host", CSRC / "chr_host.cu", ["-fmad=false"]))
     units.append(("capi", CSRC / "capi.cu", []))
     units.append(("validate", CSRC / "validate.cu", ["-fmad=false"]))

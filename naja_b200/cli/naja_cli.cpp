@@ -302,6 +302,7 @@ struct RunConfig {
               backmap_mode = "fp64";
   bool backmap = false, write_npy = false, verbose = false, quiet = false, dry_run = false, print_config = false,
        write_samples_valid = false;
+  bool tpb_set = false;  // --tpb given: run that thread count; otherwise the library picks the kernel
   std::string file(const std::string& what) const { return rounding_dir + "/" + model_name + "_rounding_" + what + ".csv"; }
 };
 
@@ -507,7 +508,7 @@ int run_sampling(const RunConfig& c) {
   p.nspc = c.n_samples;
   p.thinning = thinning;
   p.nchains = c.n_chains;
-  p.tpb = c.tpb;
+  p.tpb = c.tpb_set ? c.tpb : 0;
   p.seed = static_cast<unsigned long long>(static_cast<long long>(seed));
   p.pair_prob = c.pair_prob;
   p.resync_interval = c.resync_interval;
@@ -594,7 +595,10 @@ int cmd_sample_run(int argc, char** argv) {
     else if (a == "--gpu") c.gpu = std::stoi(next_arg(i, argc, argv, a));
     else if (a == "--n-chains") c.n_chains = std::stoi(next_arg(i, argc, argv, a));
     else if (a == "--n-samples") c.n_samples = std::stoi(next_arg(i, argc, argv, a));
-    else if (a == "--tpb") c.tpb = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--tpb") {
+      c.tpb = std::stoi(next_arg(i, argc, argv, a));
+      c.tpb_set = true;
+    }
     else if (a == "--thinning") c.thinning = std::stoi(next_arg(i, argc, argv, a));
     else if (a == "--pair-prob") c.pair_prob = std::stod(next_arg(i, argc, argv, a));
     else if (a == "--resync-interval") c.resync_interval = std::stoi(next_arg(i, argc, argv, a));

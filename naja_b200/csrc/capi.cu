@@ -8,8 +8,10 @@
 // records a thread-local message.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -125,6 +127,22 @@ int device_view(const void* p, size_t n, cudaStream_t s, DeviceBuffer& buf, cons
 
 using namespace naja;
 
+// Compressed copies of A for the sparse-column kernel, built on the first
+// run that may use them.
+struct SparseStore {
+  bool built = false;
+  long long nnz = 0;        // nonzeros of the FP64 A
+  long long tot32 = 0, tot64 = 0;  // column entries stored, padding included
+  void* cols32 = nullptr;   // (float, int) entries of A32 by columns
+  int* cs32 = nullptr;
+  int max32 = 0;
+  void* cols64 = nullptr;   // (double, int, pad) entries of A64 by columns
+  int* cs64 = nullptr;
+  int max64 = 0;
+  int* row_start = nullptr; // A64 by rows, (value, column) entries in groups of kSpRowGroup
+  void* row_ent = nullptr;
+};
+
 struct naja_polytope {
   int device = 0;
   int m = 0, d = 0, lda = 0;
@@ -132,7 +150,242 @@ struct naja_polytope {
   float* A32 = nullptr;
   double* b = nullptr;
   int* err = nullptr;
+  std::mutex sparse_mu;
+  SparseStore sp;
 };
+
+namespace sparse_build {
+
+void free_sparse(SparseStore& s) {
+  cudaFree(s.cols32);
+  cudaFree(s.cs32);
+  cudaFree(s.cols64);
+  cudaFree(s.cs64);
+  cudaFree(s.row_start);
+  cudaFree(s.row_ent);
+  s = SparseStore();
+}
+
+struct SpE32 {
+  float v;
+  int r;
+};
+struct __align__(16) SpE64 {
+  double v;
+  int r;
+  int pad;
+};
+static_assert(sizeof(SpE32) == kSpEntryBytes32 && sizeof(SpE64) == kSpEntryBytes64, "entry layout");
+
+// Entries a compressed column of n nonzeros stores: FP32 entries come in
+// pairs (16 bytes), every column holds at least one 16-byte group.
+inline int padded32(int n) { return n < 2 ? 2 : n + (n & 1); }
+inline int padded64(int n) { return n < 1 ? 1 : n; }
+
+// One warp per column: nonzeros of the FP32 and FP64 column, and per row
+// the FP64 nonzeros (for the row offsets).
+__global__ void sp_count_kernel(const double* A64, const float* A32, int m, int d, int lda, int* cnt32, int* cnt64,
+                                int* rowcnt) {
+  const int j = static_cast<int>((blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= d) return;
+  const double* c64 = A64 + static_cast<size_t>(j) * lda;
+  const float* c32 = A32 + static_cast<size_t>(j) * lda;
+  int n32 = 0, n64 = 0;
+  for (int r0 = 0; r0 < m; r0 += 32) {
+    const int r = r0 + lane;
+    const bool nz64 = r < m && c64[r] != 0.0;
+    const bool nz32 = r < m && c32[r] != 0.0f;
+    n64 += __popc(__ballot_sync(0xffffffffu, nz64));
+    n32 += __popc(__ballot_sync(0xffffffffu, nz32));
+    if (nz64) atomicAdd(&rowcnt[r], 1);
+  }
+  if (lane == 0) {
+    cnt32[j] = n32;
+    cnt64[j] = n64;
+  }
+}
+
+// One warp per column: the nonzeros in row order (ballot compaction), then
+// the (0, m) padding.
+__global__ void sp_fill_cols_kernel(const double* A64, const float* A32, int m, int d, int lda, const int* cs32,
+                                    const int* cs64, SpE32* cols32, SpE64* cols64) {
+  const int j = static_cast<int>((blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (j >= d) return;
+  const double* c64 = A64 + static_cast<size_t>(j) * lda;
+  const float* c32 = A32 + static_cast<size_t>(j) * lda;
+  const unsigned lt = (1u << lane) - 1u;
+  int p32 = cs32[j], p64 = cs64[j];
+  for (int r0 = 0; r0 < m; r0 += 32) {
+    const int r = r0 + lane;
+    const double v64 = r < m ? c64[r] : 0.0;
+    const float v32 = r < m ? c32[r] : 0.0f;
+    const unsigned b64 = __ballot_sync(0xffffffffu, v64 != 0.0);
+    const unsigned b32 = __ballot_sync(0xffffffffu, v32 != 0.0f);
+    if (v64 != 0.0) cols64[p64 + __popc(b64 & lt)] = SpE64{v64, r, 0};
+    if (v32 != 0.0f) cols32[p32 + __popc(b32 & lt)] = SpE32{v32, r};
+    p64 += __popc(b64);
+    p32 += __popc(b32);
+  }
+  for (int q = p32 + lane; q < cs32[j + 1]; q += 32) cols32[q] = SpE32{0.0f, m};
+  for (int q = p64 + lane; q < cs64[j + 1]; q += 32) cols64[q] = SpE64{0.0, m, 0};
+}
+
+// One warp per row: the FP64 nonzeros in column order, then (0, 0)
+// padding to the row's group boundary.
+__global__ void sp_fill_rows_kernel(const double* A64, int m, int d, int lda, const int* row_start, SpE64* row_ent) {
+  const int r = static_cast<int>((blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (r >= m) return;
+  const unsigned lt = (1u << lane) - 1u;
+  int p = row_start[r];
+  for (int j0 = 0; j0 < d; j0 += 32) {
+    const int j = j0 + lane;
+    const double v = j < d ? A64[r + static_cast<size_t>(j) * lda] : 0.0;
+    const unsigned bm = __ballot_sync(0xffffffffu, v != 0.0);
+    if (v != 0.0) row_ent[p + __popc(bm & lt)] = SpE64{v, j, 0};
+    p += __popc(bm);
+  }
+  for (int q = p + lane; q < row_start[r + 1]; q += 32) row_ent[q] = SpE64{0.0, 0, 0};
+}
+
+// Builds the compressed columns of both tiers (entries where the tier's A
+// is nonzero, rows ascending, padded with (0, m) entries to 16 bytes) and
+// the FP64 rows (columns ascending) from the device copies of A: counts on
+// the device, offsets on the host, entries filled by ballot compaction.
+int build_sparse(naja_polytope* P) {
+  SparseStore& S = P->sp;
+  const int m = P->m, d = P->d, lda = P->lda;
+  int* cnt = nullptr;  // cnt32[d], cnt64[d], rowcnt[m]
+  cudaError_t e = cudaMalloc(&cnt, (2 * static_cast<size_t>(d) + m) * sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(cnt, 0, (2 * static_cast<size_t>(d) + m) * sizeof(int));
+  const int col_blocks = (d + 7) / 8, row_blocks = (m + 7) / 8;
+  if (e == cudaSuccess) {
+    sp_count_kernel<<<col_blocks, 256>>>(P->A64, P->A32, m, d, lda, cnt, cnt + d, cnt + 2 * d);
+    e = cudaGetLastError();
+  }
+  std::vector<int> h(2 * static_cast<size_t>(d) + m);
+  if (e == cudaSuccess) e = cudaMemcpy(h.data(), cnt, h.size() * sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(cnt);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(NAJA_ERR_CUDA, std::string("building compressed columns: ") + cudaGetErrorString(e));
+  }
+  std::vector<int> cs32(d + 1), cs64(d + 1), rs(m + 1);
+  long long t32 = 0, t64 = 0, nnz = 0;
+  int max32 = 0, max64 = 0;
+  for (int j = 0; j < d; ++j) {
+    cs32[j] = static_cast<int>(t32);
+    cs64[j] = static_cast<int>(t64);
+    const int p32 = padded32(h[j]), p64 = padded64(h[d + j]);
+    t32 += p32;
+    t64 += p64;
+    max32 = std::max(max32, p32);
+    max64 = std::max(max64, p64);
+    if (t32 > (1LL << 30) || t64 > (1LL << 30))
+      return fail(NAJA_ERR_UNSUPPORTED, "building compressed columns: too many nonzeros");
+  }
+  cs32[d] = static_cast<int>(t32);
+  cs64[d] = static_cast<int>(t64);
+  long long nrow = 0;  // row entries, padding included
+  for (int r = 0; r < m; ++r) {
+    rs[r] = static_cast<int>(nrow);
+    nnz += h[2 * d + r];
+    nrow += (h[2 * d + r] + kSpRowGroup - 1) / kSpRowGroup * kSpRowGroup;
+    if (nrow > (1LL << 30)) return fail(NAJA_ERR_UNSUPPORTED, "building compressed rows: too many nonzeros");
+  }
+  rs[m] = static_cast<int>(nrow);
+  e = cudaMalloc(&S.cols32, static_cast<size_t>(t32) * sizeof(SpE32));
+  if (e == cudaSuccess) e = cudaMalloc(&S.cols64, static_cast<size_t>(t64) * sizeof(SpE64));
+  if (e == cudaSuccess) e = cudaMalloc(&S.cs32, (d + 1) * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&S.cs64, (d + 1) * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&S.row_start, (m + 1) * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&S.row_ent, std::max<long long>(nrow, 1) * sizeof(SpE64));
+  if (e == cudaSuccess) e = cudaMemcpy(S.cs32, cs32.data(), (d + 1) * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(S.cs64, cs64.data(), (d + 1) * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(S.row_start, rs.data(), (m + 1) * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    sp_fill_cols_kernel<<<col_blocks, 256>>>(P->A64, P->A32, m, d, lda, S.cs32, S.cs64,
+                                             static_cast<SpE32*>(S.cols32), static_cast<SpE64*>(S.cols64));
+    sp_fill_rows_kernel<<<row_blocks, 256>>>(P->A64, m, d, lda, S.row_start, static_cast<SpE64*>(S.row_ent));
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    free_sparse(S);
+    return fail(NAJA_ERR_NO_MEMORY, std::string("building compressed columns: ") + cudaGetErrorString(e));
+  }
+  S.max32 = max32;
+  S.max64 = max64;
+  S.tot32 = t32;
+  S.tot64 = t64;
+  S.nnz = nnz;
+  S.built = true;
+  return NAJA_OK;
+}
+
+}  // namespace sparse_build
+
+namespace {
+// Picks the step kernel and its launch configuration for a run (the same
+// choice for naja_chr_run and naja_chr_kernel_choice).  Compressed columns:
+// forced, or automatic when the columns are at most a quarter full on
+// average and the chain's state fits on chip.  Results are the same either
+// way.
+int choose_kernel(const naja_polytope* P, const naja_chr_params* p, ChrLaunchConfig* cfg, SpArgs* spa,
+                  bool* use_sparse) {
+  if (p->cluster < 0 || p->cluster > 8)
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run: cluster must be 0 (automatic) or 1..8");
+  if (p->sparse < NAJA_SPARSE_AUTO || p->sparse > NAJA_SPARSE_COLUMNS)
+    return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run: unknown sparse mode");
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
+  // carried MRG states are read and written by one CTA per chain
+  const int cluster_req = p->rng_state ? 1 : p->cluster;
+  std::memset(spa, 0, sizeof(*spa));
+  *use_sparse = false;
+  int st = NAJA_OK;
+  // automatic: only when the thread count is automatic too
+  const bool tpb_ok = p->tpb <= 0 || (p->sparse == NAJA_SPARSE_COLUMNS &&
+                                      (p->tpb == 32 || p->tpb == 64 || p->tpb == 128 || p->tpb == 256 ||
+                                       p->tpb == 512));
+  const bool sparse_shape = p->ksparse_prob <= 0.0 && cluster_req <= 1 && tpb_ok;
+  if (p->sparse == NAJA_SPARSE_COLUMNS && !sparse_shape)
+    return fail(NAJA_ERR_UNSUPPORTED, "naja_chr_run: compressed columns need ksparse_prob = 0, one CTA per chain "
+                                      "and tpb 0, 32, 64, 128, 256 or 512");
+  if (p->sparse != NAJA_SPARSE_DENSE && sparse_shape) {
+    naja_polytope* Pm = const_cast<naja_polytope*>(P);
+    std::lock_guard<std::mutex> lock(Pm->sparse_mu);
+    if (!Pm->sp.built && (st = sparse_build::build_sparse(Pm))) return st;
+    const SparseStore& S = Pm->sp;
+    const bool f64 = p->precision == NAJA_PREC_FP64;
+    const int max_col = f64 ? S.max64 : S.max32;
+    const long long tot = f64 ? S.tot64 : S.tot32;
+    if (p->sparse == NAJA_SPARSE_COLUMNS || 4 * tot <= static_cast<long long>(P->m) * P->d) {
+      st = chr_sparse_plan(p->precision, P->m, P->d, max_col, static_cast<double>(tot) / P->d, p->tpb,
+                           p->max_slots, cfg);
+      if (st == NAJA_OK) {
+        *use_sparse = true;
+        spa->cols = f64 ? S.cols64 : S.cols32;
+        spa->col_start = f64 ? S.cs64 : S.cs32;
+        spa->row_start = S.row_start;
+        spa->row_ent = S.row_ent;
+        return NAJA_OK;
+      }
+      if (p->sparse == NAJA_SPARSE_COLUMNS)
+        return fail(st, "naja_chr_run: the compressed columns' state (m=" + std::to_string(P->m) + ", d=" +
+                            std::to_string(P->d) + ") does not fit in shared memory");
+    }
+  }
+  st = chr_plan(p->precision, P->m, P->d, P->lda, p->tpb, p->max_slots, p->nchains, cluster_req, sms, cfg);
+  if (st == NAJA_ERR_INVALID_ARGUMENT) return fail(st, "Invalid threads per block");
+  if (st) return fail(st, "CoordinateHitAndRun: shape (m=" + std::to_string(P->m) + ", d=" + std::to_string(P->d) +
+                              ") exceeds the step kernel's capacity for this thread count");
+  return NAJA_OK;
+}
+}  // namespace
 
 extern "C" {
 
@@ -212,6 +465,7 @@ int naja_polytope_destroy(naja_polytope* P) {
   cudaFree(P->A32);
   cudaFree(P->b);
   cudaFree(P->err);
+  sparse_build::free_sparse(P->sp);
   delete P;
   return NAJA_OK;
 }
@@ -229,6 +483,23 @@ int naja_polytope_check(const naja_polytope* P) {
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_polytope_check: ") + cudaGetErrorString(e));
   return read_device_error(P->err);
+}
+
+int naja_chr_kernel_choice(const naja_polytope* P, const naja_chr_params* p, int* sparse_kernel, int* threads,
+                           int* slots, size_t* smem) {
+  if (!P || !p) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_kernel_choice: null polytope or params");
+  DeviceGuard g(P->device);
+  if (!g.ok()) return fail(NAJA_ERR_CUDA, "naja_chr_kernel_choice: cannot select device");
+  ChrLaunchConfig cfg;
+  SpArgs spa;
+  bool use_sparse = false;
+  const int st = choose_kernel(P, p, &cfg, &spa, &use_sparse);
+  if (st) return st;
+  if (sparse_kernel) *sparse_kernel = use_sparse ? 1 : 0;
+  if (threads) *threads = cfg.threads;
+  if (slots) *slots = cfg.slots;
+  if (smem) *smem = cfg.smem;
+  return NAJA_OK;
 }
 
 int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double* X0, int ldx, void* samples,
@@ -261,16 +532,10 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
 
   ChrLaunchConfig cfg;
-  if (p->cluster < 0 || p->cluster > 8)
-    return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run: cluster must be 0 (automatic) or 1..8");
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device);
-  // carried MRG states are read and written by one CTA per chain
-  const int cluster_req = p->rng_state ? 1 : p->cluster;
-  int st = chr_plan(p->precision, P->m, P->d, P->lda, p->tpb, p->max_slots, p->nchains, cluster_req, sms, &cfg);
-  if (st == NAJA_ERR_INVALID_ARGUMENT) return fail(st, "Invalid threads per block");
-  if (st) return fail(st, "CoordinateHitAndRun: shape (m=" + std::to_string(P->m) + ", d=" + std::to_string(P->d) +
-                              ") exceeds the step kernel's capacity for this thread count");
+  SpArgs spa;
+  bool use_sparse = false;
+  int st = choose_kernel(P, p, &cfg, &spa, &use_sparse);
+  if (st) return st;
 
   const int d = P->d;
   const size_t out_elt = p->out_dtype == NAJA_DTYPE_F64 ? 8 : 4;
@@ -341,7 +606,8 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
   a.timeout_ns = kWaitTimeoutNs;
   a.wait_cycles = p->wait_cycles;
 
-  st = chr_launch(p->precision, a, p->nchains, cfg, stream);
+  st = use_sparse ? chr_sparse_launch(p->precision, a, spa, p->nchains, cfg, stream)
+                  : chr_launch(p->precision, a, p->nchains, cfg, stream);
   if (st) {
     cudaError_t e = cudaGetLastError();
     return fail(st, std::string("CoordinateHitAndRun: launch failed: ") + cudaGetErrorString(e));

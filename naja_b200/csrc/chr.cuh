@@ -52,7 +52,38 @@ struct ChrLaunchConfig {
   size_t smem;    // dynamic shared memory bytes
   int cluster;    // CTAs per chain (thread-block cluster); 1 = one CTA per chain
   int slice_lda;  // rows a CTA's column slot holds (cluster > 1), padded to 32
+  int max_col;    // sparse-column kernel: entries of the longest compressed column
 };
+
+// Compressed columns of A for the sparse-column kernel, in the tier's
+// precision: column j's entries (value, row) are cols[col_start[j],
+// col_start[j + 1]), rows ascending, padded with (0, m) entries to a
+// 16-byte multiple and to at least one 16-byte group.  row_ent holds the
+// FP64 A by rows for the FP64 slack recompute: row r's (value, column)
+// entries (16 bytes each, columns ascending) are row_ent[row_start[r],
+// row_start[r + 1]), padded with (0, 0) entries to a multiple of
+// kSpRowGroup.
+struct SpArgs {
+  const void* cols;
+  const int* col_start;
+  const int* row_start;
+  const void* row_ent;
+};
+constexpr int kSpRowGroup = 16;
+
+// Entry sizes of the compressed columns: (float value, int row) and
+// (double value, int row, padding).
+constexpr int kSpEntryBytes32 = 8;
+constexpr int kSpEntryBytes64 = 16;
+
+// Plans the sparse-column kernel: `tpb` consumer threads per chain (32, 64,
+// 128, 256 or 512; <= 0 = automatic from the mean column length `mean_col`),
+// `max_col` entries per staged column.  Returns 0 or a naja status code
+// (NAJA_ERR_UNSUPPORTED when the chain's state does not fit on chip).
+int chr_sparse_plan(int precision, int m, int d, int max_col, double mean_col, int tpb, int max_slots,
+                    ChrLaunchConfig* out);
+int chr_sparse_launch(int precision, const ChrArgs& args, const SpArgs& sp, int nchains, const ChrLaunchConfig& cfg,
+                      cudaStream_t stream);
 
 // Picks a launch configuration.  `tpb` > 0 forces the consumer thread count
 // (one of the reference's 32, 64, 128, 256, 512, 1024; 1024 runs as 992 consumer

@@ -60,7 +60,8 @@ struct __align__(16) StepMeta {
   double ci;
   double cj;
   double u;
-  double pad;
+  int na;  // sparse-column kernel: entries staged in slot_a / slot_b
+  int nb;
   int ks_idx[32];
   double ks_coef[32];
 };
@@ -94,6 +95,8 @@ struct Layout {
   size_t x_off, slot_off, slot_bytes, meta_off, full_off, empty_off, red_off, flag_off, tail_off, slack_off, total;
   int slots;
   bool direct;
+  // sparse-column kernel only: column offsets and the pair-step scratch column
+  size_t cs_off, ajd_off;
 };
 
 // slack_rows > 0 reserves a shared-memory slack store (slack_rows values of
@@ -129,6 +132,7 @@ __host__ __device__ inline Layout make_layout(int d, int lda, int elt, int nthre
   L.total = align_up(off, 128);
   L.slots = S;
   L.direct = direct;
+  L.cs_off = L.ajd_off = 0;
   return L;
 }
 
@@ -377,8 +381,12 @@ struct Tier<double> {
 // One thread: draws each step's direction ahead of the consumers, claims one
 // ring slot per staged column (two for a pair step, one metadata-only slot
 // for a k-sparse step), writes the step record and starts the bulk copy.
-template <class Real, class Src>
-__device__ __noinline__ void run_producer(const ChrArgs& a, Src& src, const Layout& L, unsigned char* smem) {
+// SPARSE: the slot receives the column's compressed entries (offsets from
+// the shared copy `cs` of col_start, entry size `eb`) and the record their
+// count.
+template <class Real, class Src, bool SPARSE = false>
+__device__ __noinline__ void run_producer(const ChrArgs& a, Src& src, const Layout& L, unsigned char* smem,
+                                          const SpArgs* sp = nullptr, const int* cs = nullptr, int eb = 0) {
   StepMeta* meta = reinterpret_cast<StepMeta*>(smem + L.meta_off);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);
   uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
@@ -460,7 +468,23 @@ __device__ __noinline__ void run_producer(const ChrArgs& a, Src& src, const Layo
       used_mask |= 1u << sb;
       last_parity = (last_parity & ~(1u << sb)) | ((rb & 1u) << sb);
     }
-    if (!L.direct && dir.kind != kKSparse) {
+    if constexpr (SPARSE) {
+      // every column holds at least one 16-byte group of entries
+      const unsigned char* cols = static_cast<const unsigned char*>(sp->cols);
+      const int s0 = cs[dir.ei], n0 = cs[dir.ei + 1] - s0;
+      M.na = n0;
+      M.nb = 0;
+      if (sb >= 0) M.nb = cs[dir.ej + 1] - cs[dir.ej];
+      mbar_arrive_expect_tx(&full[sa], static_cast<uint32_t>(n0 * eb));
+      bulk_g2s(smem + L.slot_off + static_cast<size_t>(sa) * L.slot_bytes, cols + static_cast<size_t>(s0) * eb,
+               static_cast<uint32_t>(n0 * eb), &full[sa]);
+      if (sb >= 0) {
+        const int s1 = cs[dir.ej];
+        mbar_arrive_expect_tx(&full[sb], static_cast<uint32_t>(M.nb * eb));
+        bulk_g2s(smem + L.slot_off + static_cast<size_t>(sb) * L.slot_bytes, cols + static_cast<size_t>(s1) * eb,
+                 static_cast<uint32_t>(M.nb * eb), &full[sb]);
+      }
+    } else if (!L.direct && dir.kind != kKSparse) {
       mbar_arrive_expect_tx(&full[sa], col_bytes);
       bulk_g2s(smem + L.slot_off + static_cast<size_t>(sa) * L.slot_bytes, A + static_cast<size_t>(dir.ei) * a.lda,
                col_bytes, &full[sa]);
@@ -486,15 +510,16 @@ __device__ __noinline__ void run_producer(const ChrArgs& a, Src& src, const Layo
   }
 }
 
-template <class Real>
-__device__ __noinline__ void producer_entry(const ChrArgs& a, const Layout& L, unsigned char* smem, int chain_local) {
+template <class Real, bool SPARSE = false>
+__device__ __noinline__ void producer_entry(const ChrArgs& a, const Layout& L, unsigned char* smem, int chain_local,
+                                            const SpArgs* sp = nullptr, const int* cs = nullptr, int eb = 0) {
   const int gchain = a.chain_base + chain_local;
   if (a.rng == 0) {
     PhiloxSource src;
     src.k0 = static_cast<uint32_t>(a.seed);
     src.k1 = static_cast<uint32_t>(a.seed >> 32);
     src.chain = static_cast<uint32_t>(gchain);
-    run_producer<Real>(a, src, L, smem);
+    run_producer<Real, PhiloxSource, SPARSE>(a, src, L, smem, sp, cs, eb);
   } else {
     MrgSource src;
     curandStateMRG32k3a* states = reinterpret_cast<curandStateMRG32k3a*>(a.rng_state);
@@ -503,7 +528,7 @@ __device__ __noinline__ void producer_entry(const ChrArgs& a, const Layout& L, u
     } else {
       curand_init(a.seed, static_cast<unsigned long long>(gchain), 0ull, &src.st);
     }
-    run_producer<Real>(a, src, L, smem);
+    run_producer<Real, MrgSource, SPARSE>(a, src, L, smem, sp, cs, eb);
     if (states) states[chain_local] = src.st;
   }
 }

@@ -1,0 +1,452 @@
+// Sparse-column CHR step kernel for sm_100a.
+//
+// Same steps, same arithmetic and the same results as chr_kernel (the
+// reference's chrKernel, src/gpu/chr.cu:232-490 of quothbonney/naja), for
+// constraint matrices whose columns are mostly zero: a step touches only
+// the rows where its direction's column(s) of A are nonzero.
+//
+//   * The producer stages a column's compressed entries (value, row) into
+//     the slot ring instead of the whole column.
+//   * NW consumer warps per chain (1..16); entry e of a staged column goes to
+//     consumer thread e % (32 NW).  The slack vector (m values, plus a
+//     scratch row m that padding entries point at) lives in shared memory.
+//     A step synchronises at one barrier after the column wait (every warp
+//     agrees the column arrived; the previous step's slack writes become
+//     visible) and one for the cross-warp max / min, plus two inside a pair
+//     step.  With one warp every barrier is a __syncwarp.
+//   * The chord ends are max / min over all m rows of ae/s.  A row with
+//     ae = 0 contributes a signed zero (FP32 tier: +0; FP64 tier: +-0 by the
+//     signs of ae and s), so when the extremes over the nonzero rows are
+//     strictly positive (max) and strictly negative (min) the zero rows
+//     cannot change them and the compressed pass is exact.  Otherwise (an
+//     unbounded or degenerate chord) the step repeats the pass over all m
+//     rows from the dense A.
+//   * Slack rows with ae = 0 are not updated: s - alpha * (+-0) equals s
+//     except for the sign of a zero slack, which neither tier's ratio
+//     reads (a zero slack counts as +0) and which no later update can turn
+//     into a different nonzero value.
+//   * Pair steps combine the two columns through a dense scratch column
+//     `ajd` (all zeros between steps): column j is scattered into it, the
+//     pass over column i's entries reads a_j there (0 where column j has no
+//     entry) and marks the shared rows, the pass over column j's entries
+//     skips the marked rows and clears the scratch.  ae = fma(a_i, c_i,
+//     a_j c_j) exactly as the dense kernel forms it.  The combined values
+//     go to a shared array beside the slots; the staged slots are only read.
+//   * The FP64 recompute slack = b - A64 x runs over the rows of A64
+//     stored by rows, columns ascending: the dense kernel's fma chain
+//     without its zero terms (padding terms 0 * x_0 change at most the sign
+//     of a zero sum), kSpRowGroup 16-byte entries loaded ahead of each
+//     group of as many fmas.
+#pragma once
+#include "chr_kernel.cuh"
+
+namespace naja {
+namespace chr_detail {
+namespace {
+
+template <class Real>
+struct SpEntry;
+template <>
+struct __align__(8) SpEntry<float> {
+  float v;
+  int r;
+};
+template <>
+struct __align__(16) SpEntry<double> {
+  double v;
+  int r;
+  int pad;
+};
+static_assert(sizeof(SpEntry<float>) == kSpEntryBytes32, "FP32 entry size");
+static_assert(sizeof(SpEntry<double>) == kSpEntryBytes64, "FP64 entry size");
+
+// Marker for a row shared by both columns of a pair step: -0, which no
+// stored entry holds (stored values are nonzero).
+__device__ __forceinline__ float sp_mark(float) { return __uint_as_float(0x80000000u); }
+__device__ __forceinline__ double sp_mark(double) {
+  return __longlong_as_double(static_cast<long long>(0x8000000000000000ull));
+}
+__device__ __forceinline__ bool sp_is_mark(float v) { return __float_as_uint(v) == 0x80000000u; }
+__device__ __forceinline__ bool sp_is_mark(double v) {
+  return static_cast<unsigned long long>(__double_as_longlong(v)) == 0x8000000000000000ull;
+}
+
+// Shared memory of one chain: x (FP64), the column offsets, `slots` staged
+// compressed columns of up to max_col entries, the step records and
+// barriers, the cross-warp reduction entries, the abort flag followed by the
+// arrival flags (2 x nw ints), slack and the pair scratch column (m + 1
+// values each), and a pair step's combined values (tail_off: one value per
+// slot entry for column i's entries, then as many for column j's).
+__host__ __device__ inline Layout make_sparse_layout(int d, int m, int elt, int eb, int max_col, int nw, int slots) {
+  Layout L;
+  size_t off = 0;
+  L.x_off = 0;
+  off = align_up(static_cast<size_t>(d) * 8, 128);
+  L.cs_off = off;
+  off = align_up(off + static_cast<size_t>(d + 1) * 4, 128);
+  L.slot_off = off;
+  L.slot_bytes = align_up(static_cast<size_t>(max_col) * eb, 128);
+  off += L.slot_bytes * slots;
+  L.meta_off = off;
+  off = align_up(off + sizeof(StepMeta) * slots, 16);
+  L.full_off = off;
+  off += 8 * static_cast<size_t>(slots);
+  L.empty_off = off;
+  off += 8 * static_cast<size_t>(slots);
+  L.red_off = align_up(off, 16);
+  off = L.red_off + sizeof(RedEntry) * 2 * nw;
+  L.flag_off = align_up(off, 16);
+  off = L.flag_off + 16 + 2 * static_cast<size_t>(nw) * 4;
+  L.slack_off = align_up(off, 128);
+  off = L.slack_off + static_cast<size_t>(m + 1) * elt;
+  L.ajd_off = align_up(off, 16);
+  off = L.ajd_off + static_cast<size_t>(m + 1) * elt;
+  L.tail_off = align_up(off, 16);
+  off = L.tail_off + 2 * (L.slot_bytes / eb) * elt;
+  L.total = align_up(off, 128);
+  L.slots = slots;
+  L.direct = false;
+  return L;
+}
+
+// Barrier over the consumer warps (the producer warp never takes part).
+template <int NW>
+__device__ __forceinline__ void consumers_sync(uint32_t id) {
+  if constexpr (NW == 1) {
+    __syncwarp();
+  } else {
+    named_bar_sync(id, NW * 32);
+  }
+}
+
+// The consumer warps of one chain.
+template <class Real, int NW>
+__device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const Layout& L, unsigned char* smem,
+                                     int chain_local) {
+  using T = Tier<Real>;
+  using Acc = typename T::Acc;
+  using UT = typename T::UType;
+  using E = SpEntry<Real>;
+  using R64 = SpEntry<double>;
+  constexpr int NT = 32 * NW;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  double* xs = reinterpret_cast<double*>(smem + L.x_off);
+  const StepMeta* meta = reinterpret_cast<const StepMeta*>(smem + L.meta_off);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);
+  uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
+  RedEntry* red = reinterpret_cast<RedEntry*>(smem + L.red_off);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.flag_off);
+  int* arrived = reinterpret_cast<int*>(smem + L.flag_off + 16);
+  Real* slack = reinterpret_cast<Real*>(smem + L.slack_off);
+  Real* ajd = reinterpret_cast<Real*>(smem + L.ajd_off);
+  Real* pv = reinterpret_cast<Real*>(smem + L.tail_off);  // combined values, column i's entries
+  Real* qv = pv + L.slot_bytes / sizeof(E);                 // ... column j's entries
+  const Real* A = T::A(a);
+  const R64* rows = static_cast<const R64*>(sp.row_ent);
+  const int m = a.m, d = a.d, lda = a.lda, S = L.slots;
+  const int gchain = a.chain_base + chain_local;
+
+  for (int j = tid; j < d; j += NT) xs[j] = a.X0[static_cast<size_t>(chain_local) * a.ldx + j];
+  for (int r = tid; r <= m; r += NT) ajd[r] = Real(0);
+  consumers_sync<NW>(1);
+
+  auto recompute = [&]() {
+    for (int r = tid; r < m; r += NT) {
+      double acc = 0.0;
+      const int k1 = sp.row_start[r + 1];
+      for (int k = sp.row_start[r]; k < k1; k += kSpRowGroup) {
+        R64 e[kSpRowGroup];
+#pragma unroll
+        for (int u = 0; u < kSpRowGroup; ++u) e[u] = rows[k + u];
+        double xv[kSpRowGroup];
+#pragma unroll
+        for (int u = 0; u < kSpRowGroup; ++u) xv[u] = xs[e[u].r];
+#pragma unroll
+        for (int u = 0; u < kSpRowGroup; ++u) acc = __fma_rn(e[u].v, xv[u], acc);
+      }
+      slack[r] = T::from64(__dsub_rn(a.b[r], acc));
+    }
+    if (tid == 0) slack[m] = Real(0);
+  };
+  recompute();
+  consumers_sync<NW>(1);
+
+  // Cross-warp max / min: lane 0 of each warp posts, one barrier, every
+  // warp reduces the posted entries.  The halves of `red` alternate.
+  int rbuf = 0;
+  auto reduce = [&](Acc& hi, Acc& lo, Acc& lo2) {
+    hi = T::red_hi(hi);
+    lo = T::red_lo(lo);
+    lo2 = T::red_lo2(lo2);
+    if constexpr (NW > 1) {
+      RedEntry* slotr = red + rbuf * NW;
+      rbuf ^= 1;
+      if (lane == 0) {
+        slotr[warp].kmax = hi;
+        slotr[warp].kmin = lo;
+        slotr[warp].kmin2 = lo2;
+      }
+      named_bar_sync(1, NT);
+      Acc h = T::acc_hi0(), l = T::acc_lo0(), l2 = T::acc_lo20();
+      if (lane < NW) {
+        h = static_cast<Acc>(slotr[lane].kmax);
+        l = static_cast<Acc>(slotr[lane].kmin);
+        l2 = static_cast<Acc>(slotr[lane].kmin2);
+      }
+      hi = T::red_hi(h);
+      lo = T::red_lo(l);
+      lo2 = T::red_lo2(l2);
+    }
+  };
+
+  const long long total = static_cast<long long>(a.nspc) * a.thinning;
+  int slot = 0;
+  uint32_t parity = 0;
+  // the recompute above is step 0's: the next one falls at t = resync
+  int thin_ctr = 0, resync_ctr = a.resync > 1 ? 1 : 0, abuf = 0;
+  size_t out_row = static_cast<size_t>(gchain);
+  unsigned long long w_full = 0;
+  const unsigned long long c_start = clock64();
+  for (long long t = 0; t < total; ++t) {
+    const int sa = slot;
+    const unsigned long long w0 = a.wait_cycles ? clock64() : 0ull;
+    bool ok = mbar_wait_bounded(&full[sa], parity, a.timeout_ns);
+    if (a.wait_cycles) w_full += clock64() - w0;
+    int kind = kCoord, ei = 0, ej = 0, sb = -1, na = 0, nb = 0;
+    Real cir = Real(1), cjr = Real(0);
+    UT uu = UT(0.5);
+    double cix = 1.0, cjx = 0.0;
+    if (ok) {
+      const StepMeta& M = meta[sa];
+      const int4 h0 = *reinterpret_cast<const int4*>(&M.kind);
+      const int4 h1 = *reinterpret_cast<const int4*>(&M.k);
+      const int2 hn = *reinterpret_cast<const int2*>(&M.na);
+      kind = h0.x;
+      ei = h0.y;
+      ej = h0.z;
+      sb = h0.w;
+      na = hn.x;
+      nb = hn.y;
+      if constexpr (sizeof(Real) == 4) {
+        cir = __int_as_float(h1.y);
+        cjr = __int_as_float(h1.z);
+        uu = __int_as_float(h1.w);
+        cix = static_cast<double>(cir);
+        cjx = static_cast<double>(cjr);
+      } else {
+        cir = M.ci;
+        cjr = M.cj;
+        uu = M.u;
+        cix = cir;
+        cjx = cjr;
+      }
+      if (++slot == S) {
+        slot = 0;
+        parity ^= 1u;
+      }
+      if (kind == kPair) {
+        ok = mbar_wait_bounded(&full[sb], parity, a.timeout_ns);
+        if (++slot == S) {
+          slot = 0;
+          parity ^= 1u;
+        }
+      }
+    }
+    // Every warp agrees that the step's columns arrived before any barrier
+    // that depends on the step's kind; this barrier also publishes the
+    // previous step's slack writes.
+    ok = __all_sync(0xffffffffu, ok);
+    if constexpr (NW > 1) {
+      int* af = arrived + abuf * NW;
+      abuf ^= 1;
+      if (lane == 0) af[warp] = ok ? 1 : 0;
+      named_bar_sync(3, NT);
+      ok = __all_sync(0xffffffffu, lane >= NW || af[lane] != 0);
+    }
+    if (!ok) {
+      if (tid == 0) {
+        set_error(a.err, kDevTimeoutFull, sa, static_cast<int>(parity), static_cast<int>(t));
+        *abort_flag = 1;
+      }
+      return;
+    }
+    if (a.resync > 0) {
+      if (resync_ctr == 0) {
+        recompute();
+        consumers_sync<NW>(2);
+      }
+      if (++resync_ctr == a.resync) resync_ctr = 0;
+    }
+    const E* ea = reinterpret_cast<const E*>(smem + L.slot_off + static_cast<size_t>(sa) * L.slot_bytes);
+    const E* eb =
+        reinterpret_cast<const E*>(smem + L.slot_off + static_cast<size_t>(sb < 0 ? 0 : sb) * L.slot_bytes);
+    Acc hi = T::acc_hi0(), lo = T::acc_lo0(), lo2 = T::acc_lo20();
+    if (kind == kPair) {
+#pragma unroll 4
+      for (int e = tid; e < nb; e += NT) {
+        const E q = eb[e];
+        ajd[q.r] = q.v;
+      }
+      consumers_sync<NW>(3);
+#pragma unroll 4
+      for (int e = tid; e < na; e += NT) {
+        const E q = ea[e];
+        const Real w = ajd[q.r];
+        const Real ae = T::pair_ae_r(q.v, w, cir, cjr);
+        if (w != Real(0)) ajd[q.r] = sp_mark(Real(0));
+        pv[e] = ae;
+        T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
+      }
+      consumers_sync<NW>(3);
+#pragma unroll 4
+      for (int e = tid; e < nb; e += NT) {
+        const E q = eb[e];
+        const Real w = ajd[q.r];
+        ajd[q.r] = Real(0);
+        // a row shared with column i was taken with that entry: the marker
+        // (-0) makes this entry's update a no-op below
+        Real ae = sp_mark(Real(0));
+        if (!sp_is_mark(w)) {
+          ae = T::pair_ae_r(Real(0), q.v, cir, cjr);
+          T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
+        }
+        qv[e] = ae;
+      }
+    } else {
+#pragma unroll 4
+      for (int e = tid; e < na; e += NT) {
+        const E q = ea[e];
+        T::acc(hi, lo, lo2, T::ratio(q.v, slack[q.r]));
+      }
+    }
+    reduce(hi, lo, lo2);
+    Real mx, mn;
+    T::decode(hi, lo, lo2, mx, mn);
+    if (!(mx > Real(0) && mn < Real(0))) {
+      // Some zero row may hold an extreme: repeat the pass over all rows.
+      hi = T::acc_hi0();
+      lo = T::acc_lo0();
+      lo2 = T::acc_lo20();
+      const Real* ca = A + static_cast<size_t>(ei) * lda;
+      if (kind == kPair) {
+        const Real* cb = A + static_cast<size_t>(ej) * lda;
+        for (int r = tid; r < m; r += NT) T::acc(hi, lo, lo2, T::ratio(T::pair_ae_r(ca[r], cb[r], cir, cjr), slack[r]));
+      } else {
+        for (int r = tid; r < m; r += NT) T::acc(hi, lo, lo2, T::ratio(ca[r], slack[r]));
+      }
+      reduce(hi, lo, lo2);
+      T::decode(hi, lo, lo2, mx, mn);
+    }
+    const Real alpha = T::alpha(mx, mn, uu);
+    const double a64 = static_cast<double>(alpha);
+    if (kind == kCoord) {
+      if (ei % NT == tid) xs[ei] = __dadd_rn(xs[ei], a64);
+    } else {
+      if (ei % NT == tid) xs[ei] = __fma_rn(a64, cix, xs[ei]);
+      if (ej % NT == tid) xs[ej] = __fma_rn(a64, cjx, xs[ej]);
+    }
+    if (thin_ctr == 0 && a.samples) {
+      if (a.out_f64) {
+        double* out = reinterpret_cast<double*>(a.samples) + out_row * d;
+        for (int j = tid; j < d; j += NT) out[j] = xs[j];
+      } else {
+        float* out = reinterpret_cast<float*>(a.samples) + out_row * d;
+        for (int j = tid; j < d; j += NT) out[j] = __double2float_rn(xs[j]);
+      }
+      out_row += static_cast<size_t>(a.out_nchains);
+    }
+    if (++thin_ctr == a.thinning) thin_ctr = 0;
+    // Slack update of the rows the step touched, each by the thread that
+    // read its entry.  A pair step's rows take the combined values; an entry
+    // holding the marker (a row already updated through column i, or a
+    // combined value of -0, whose update would only change the sign of a
+    // zero slack) is skipped.
+    if (kind == kPair) {
+#pragma unroll 4
+      for (int e = tid; e < na; e += NT) {
+        const int r = ea[e].r;
+        slack[r] = T::slack_update(slack[r], alpha, pv[e]);
+      }
+#pragma unroll 4
+      for (int e = tid; e < nb; e += NT) {
+        const Real ae = qv[e];
+        if (!sp_is_mark(ae)) {
+          const int r = eb[e].r;
+          slack[r] = T::slack_update(slack[r], alpha, ae);
+        }
+      }
+    } else {
+#pragma unroll 4
+      for (int e = tid; e < na; e += NT) {
+        const E q = ea[e];
+        slack[q.r] = T::slack_update(slack[q.r], alpha, q.v);
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      mbar_arrive(&empty[sa]);
+      if (kind == kPair) mbar_arrive(&empty[sb]);
+    }
+  }
+  if (a.X_final) {
+    for (int j = tid; j < d; j += NT) a.X_final[static_cast<size_t>(chain_local) * a.ldx + j] = xs[j];
+  }
+  if (a.wait_cycles && tid == 0) {
+    a.wait_cycles[4 * chain_local + 0] = w_full;
+    a.wait_cycles[4 * chain_local + 2] = clock64() - c_start;
+  }
+}
+
+template <class Real, int NW>
+__global__ void __launch_bounds__(NW * 32 + 32, 1)
+    chr_sparse_kernel(const __grid_constant__ ChrArgs a, const __grid_constant__ SpArgs sp,
+                      const __grid_constant__ Layout L) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  constexpr int NT = NW * 32;
+  int* cs = reinterpret_cast<int*>(smem + L.cs_off);
+  if (threadIdx.x == 0) {
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);
+    uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
+    for (int s = 0; s < L.slots; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], NW);
+    }
+    *reinterpret_cast<volatile int*>(smem + L.flag_off) = 0;
+    fence_mbar_init();
+  }
+  for (int j = threadIdx.x; j <= a.d; j += blockDim.x) cs[j] = sp.col_start[j];
+  __syncthreads();
+  if (threadIdx.x >= NT) {
+    if (threadIdx.x == NT)
+      producer_entry<Real, true>(a, L, smem, blockIdx.x, &sp, cs, static_cast<int>(sizeof(SpEntry<Real>)));
+    return;
+  }
+  run_sparse_consumers<Real, NW>(a, sp, L, smem, blockIdx.x);
+}
+
+template <class Real, int NW>
+int launch_sparse(const ChrArgs& a, const SpArgs& sp, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream) {
+  auto kern = chr_sparse_kernel<Real, NW>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(cfg.smem));
+  if (e != cudaSuccess) return NAJA_ERR_CUDA;
+  const Layout L = make_sparse_layout(a.d, a.m, sizeof(Real), sizeof(SpEntry<Real>), cfg.max_col, NW, cfg.slots);
+  kern<<<nchains, NW * 32 + 32, cfg.smem, stream>>>(a, sp, L);
+  return cudaGetLastError() == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
+}
+
+template <class Real>
+int launch_sparse_nw(const ChrArgs& a, const SpArgs& sp, int nchains, const ChrLaunchConfig& cfg,
+                     cudaStream_t stream) {
+  switch (cfg.threads) {
+    case 32: return launch_sparse<Real, 1>(a, sp, nchains, cfg, stream);
+    case 64: return launch_sparse<Real, 2>(a, sp, nchains, cfg, stream);
+    case 128: return launch_sparse<Real, 4>(a, sp, nchains, cfg, stream);
+    case 256: return launch_sparse<Real, 8>(a, sp, nchains, cfg, stream);
+    case 512: return launch_sparse<Real, 16>(a, sp, nchains, cfg, stream);
+    default: return NAJA_ERR_UNSUPPORTED;
+  }
+}
+
+}  // namespace
+}  // namespace chr_detail
+}  // namespace naja

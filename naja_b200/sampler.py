@@ -24,6 +24,7 @@ except Exception:  # pragma: no cover - torch is present in this image
 
 _PREC = {"fp32": _lib.PREC_FP32, "fp64": _lib.PREC_FP64}
 _RNG = {"philox": _lib.RNG_PHILOX, "mrg": _lib.RNG_REF_MRG, "ref_mrg": _lib.RNG_REF_MRG}
+_SPARSE = {"auto": _lib.SPARSE_AUTO, "dense": _lib.SPARSE_DENSE, "columns": _lib.SPARSE_COLUMNS}
 _BACKMAP = {"fp64": _lib.BACKMAP_FP64, "bf16x3": _lib.BACKMAP_BF16X3, "tf32x3": _lib.BACKMAP_TF32X3}
 
 
@@ -105,7 +106,7 @@ class Polytope:
     def params(self, nspc, thinning, nchains, *, tpb=-1, seed=0, pair_prob=0.0, resync_interval=0,
                ksparse_prob=0.0, ksparse_k=8, pair_mode=1, pairs=None, precision="fp32", rng="philox",
                out_dtype="f32", chain_base=0, out_nchains=0, step_offset=0, max_slots=0, rng_state=None,
-               wait_cycles=None, cluster=0):
+               wait_cycles=None, cluster=0, sparse="auto"):
         p = ChrParams()
         load().naja_chr_params_default(C.byref(p))
         p.nspc, p.thinning, p.nchains, p.tpb = int(nspc), int(thinning), int(nchains), int(tpb)
@@ -134,7 +135,18 @@ class Polytope:
         if wait_cycles is not None:
             p.wait_cycles = _ptr(wait_cycles).value
         p.cluster = int(cluster)
+        p.sparse = _SPARSE[sparse]
         return p, keep
+
+    def kernel_choice(self, nspc, thinning, nchains, **kw):
+        """The step kernel a run with these arguments launches:
+        dict(kernel="columns" | "dense", threads, slots, smem)."""
+        p, keep = self.params(nspc, thinning, nchains, **kw)
+        sk, th, sl, sm = C.c_int(), C.c_int(), C.c_int(), C.c_size_t()
+        check(load().naja_chr_kernel_choice(self._h, C.byref(p), C.byref(sk), C.byref(th), C.byref(sl), C.byref(sm)))
+        del keep
+        return {"kernel": "columns" if sk.value else "dense", "threads": th.value, "slots": sl.value,
+                "smem": sm.value}
 
     def run(self, X0, nspc, thinning, nchains=None, *, out=None, X_final=None, stream=None, **kw):
         """Runs the chains; returns the (nspc*out_nchains, d) sample matrix.
