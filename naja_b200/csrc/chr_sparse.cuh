@@ -202,8 +202,7 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
   const long long total = static_cast<long long>(a.nspc) * a.thinning;
   int slot = 0;
   uint32_t parity = 0;
-  // the recompute above is step 0's: the next one falls at t = resync
-  int thin_ctr = 0, resync_ctr = a.resync > 1 ? 1 : 0, abuf = 0;
+  int thin_ctr = 0, resync_ctr = 0, abuf = 0;
   size_t out_row = static_cast<size_t>(gchain);
   unsigned long long w_full = 0;
   const unsigned long long c_start = clock64();
@@ -271,7 +270,8 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
       return;
     }
     if (a.resync > 0) {
-      if (resync_ctr == 0) {
+      // the recompute before the loop is step 0's
+      if (resync_ctr == 0 && t != 0) {
         recompute();
         consumers_sync<NW>(2);
       }
