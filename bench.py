@@ -395,10 +395,9 @@ def _batched(a, torch, dev):
     outs = [torch.empty((nspc * nch, a.d), dtype=torch.float32, device=dev) for _ in polys]
     kw = dict(seed=a.seed, pair_prob=a.pair_prob, resync_interval=a.resync)
     if a.batch_shape:
-        t_, s_, ss_, c_ = (int(v) for v in a.batch_shape.split(","))
         from naja_b200.batch import Shape
 
-        shape, table = Shape(t_, s_, ss_, c_), {}
+        shape, table = Shape(*(int(v) for v in a.batch_shape.split(","))), {}
     else:
         shape, table = autotune.tune(B, X, outs, nch, thin, **kw)
     g = B.capture(X, outs, nspc, thin, nch, shape=shape, **kw)
@@ -627,7 +626,7 @@ def main(argv=None):
     ap.add_argument("--batch-models", type=int, default=64, help="batched-variant section (0 = skip)")
     ap.add_argument("--batch-chains", type=int, default=8)
     ap.add_argument("--batch-nspc", type=int, default=4000)
-    ap.add_argument("--batch-shape", default="", help="threads,slots,slack_smem,ctas_per_sm (skips the autotuner)")
+    ap.add_argument("--batch-shape", default="", help="threads,slots,slack_smem,ctas_per_sm[,sparse] (skips the autotuner)")
     ap.add_argument("--ref-budget-s", type=float, default=200.0,
                     help="reference arm: time budget of the K timed steps")
     ap.add_argument("--ref-cpu", action="store_true", help="reference arm: time the CPU restatement")

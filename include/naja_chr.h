@@ -145,6 +145,8 @@ typedef struct naja_batch_config {
     int slots;        /* staged-column ring depth 2..8, 0 = direct column reads */
     int slack_smem;   /* 1: slack in shared memory (several chains per SM)      */
     int ctas_per_sm;  /* resident chains per SM, 0 = as many as fit             */
+    int sparse;       /* 1: compressed-column kernel (threads 64, 128 or 256 consumer
+                         threads, slots 3..8, slack_smem ignored); same samples       */
 } naja_batch_config;
 
 /* Runs params->nchains chains of each of `nmodels` polytopes (the same d)

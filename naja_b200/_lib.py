@@ -121,7 +121,8 @@ class ChrParams(C.Structure):
 class BatchConfig(C.Structure):
     """Mirror of `naja_batch_config`."""
 
-    _fields_ = [("threads", C.c_int), ("slots", C.c_int), ("slack_smem", C.c_int), ("ctas_per_sm", C.c_int)]
+    _fields_ = [("threads", C.c_int), ("slots", C.c_int), ("slack_smem", C.c_int), ("ctas_per_sm", C.c_int),
+                ("sparse", C.c_int)]
 
 
 class NajaError(RuntimeError):

@@ -20,17 +20,28 @@ SLOTS = (0, 2, 3, 4)
 CTAS = (0, 1, 2, 3, 4)
 
 
+SPARSE_THREADS = (64, 128, 256)
+SPARSE_SLOTS = (3, 4, 8)
+
+
+def _shapes():
+    for t, s, ss, c in itertools.product(THREADS, SLOTS, (1, 0), CTAS):
+        yield Shape(t, s, ss, c)
+    for t, s, c in itertools.product(SPARSE_THREADS, SPARSE_SLOTS, CTAS):
+        yield Shape(t, s, 1, c, sparse=1)
+
+
 def candidates(batch: Batch):
     seen = set()
-    for t, s, ss, c in itertools.product(THREADS, SLOTS, (1, 0), CTAS):
-        shape = Shape(t, s, ss, c)
+    for shape in _shapes():
+        t, s, ss, c = shape.threads, shape.slots, shape.slack_smem, shape.ctas_per_sm
         try:
             occ = batch.occupancy(shape)
         except NajaError:  # no instantiated capacity holds these models
             continue
         if occ == 0:
             continue
-        eff = (t, s, ss, min(c, occ) if c else occ)
+        eff = (t, s, ss, min(c, occ) if c else occ, shape.sparse)
         if eff in seen:
             continue
         seen.add(eff)

@@ -28,9 +28,10 @@ class Shape:
     slots: int = 3
     slack_smem: int = 1
     ctas_per_sm: int = 0
+    sparse: int = 0  # 1: compressed-column kernel (threads 64 / 128 / 256)
 
     def c(self) -> BatchConfig:
-        return BatchConfig(self.threads, self.slots, self.slack_smem, self.ctas_per_sm)
+        return BatchConfig(self.threads, self.slots, self.slack_smem, self.ctas_per_sm, self.sparse)
 
 
 class Batch:

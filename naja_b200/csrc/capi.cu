@@ -668,6 +668,24 @@ struct BatchPrep {
   int device = 0;
 };
 
+// Builds every model's compressed columns (once per polytope) and records
+// the longest FP32 column for a compressed-column batch.
+int batch_sparse_prepare(int nmodels, const naja_polytope* const* models, BatchConfig* cfg) {
+  int max_col = 0;
+  for (int k = 0; k < nmodels; ++k) {
+    naja_polytope* Pm = const_cast<naja_polytope*>(models[k]);
+    if (!Pm) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: null model");
+    std::lock_guard<std::mutex> lock(Pm->sparse_mu);
+    DeviceGuard g(Pm->device);
+    int st = NAJA_OK;
+    if (!Pm->sp.built && (st = sparse_build::build_sparse(Pm))) return st;
+    max_col = std::max(max_col, Pm->sp.max32);
+  }
+  cfg->sparse = 1;
+  cfg->max_col = max_col;
+  return NAJA_OK;
+}
+
 int prep_batch(int nmodels, const naja_polytope* const* models, const naja_chr_params* p, const double* const* X0s,
                int ldx, void* const* samples, unsigned long long seed_stride, const naja_batch_config* c,
                BatchPrep* out) {
@@ -704,7 +722,13 @@ int prep_batch(int nmodels, const naja_polytope* const* models, const naja_chr_p
   cfg.slots = c->slots;
   cfg.slack_smem = c->slack_smem;
   cfg.ctas_per_sm = c->ctas_per_sm;
-  int st = chr_batch_plan(m_max, d, lda_max, &cfg);
+  int st = NAJA_OK;
+  if (c->sparse) {
+    if (p->ksparse_prob > 0.0)
+      return fail(NAJA_ERR_UNSUPPORTED, "naja_chr_run_batched: compressed columns need ksparse_prob = 0");
+    if ((st = batch_sparse_prepare(nmodels, models, &cfg))) return st;
+  }
+  st = chr_batch_plan(m_max, d, lda_max, &cfg);
   if (st == NAJA_ERR_INVALID_ARGUMENT) return fail(st, "naja_chr_run_batched: bad batch configuration");
   if (st) return fail(st, "naja_chr_run_batched: configuration cannot hold models of " + std::to_string(m_max) + " rows");
   ChrArgs& a = out->base;
@@ -745,6 +769,13 @@ int prep_batch(int nmodels, const naja_polytope* const* models, const naja_chr_p
     m.samples = samples[k];
     m.X_final = nullptr;
     m.seed = p->seed + static_cast<unsigned long long>(k) * seed_stride;
+    std::memset(&m.sp, 0, sizeof(m.sp));
+    if (cfg.sparse) {
+      m.sp.cols = P->sp.cols32;
+      m.sp.col_start = P->sp.cs32;
+      m.sp.row_start = P->sp.row_start;
+      m.sp.row_ent = P->sp.row_ent;
+    }
   }
   // chains of different models interleave, so resident CTAs spread over models
   for (int ch = 0; ch < p->nchains; ++ch)
@@ -821,6 +852,10 @@ extern "C" int naja_batch_occupancy(int nmodels, const naja_polytope* const* mod
   cfg.slack_smem = c->slack_smem;
   cfg.ctas_per_sm = c->ctas_per_sm;
   *ctas_per_sm = 0;
+  if (c->sparse) {
+    const int st = batch_sparse_prepare(nmodels, models, &cfg);
+    if (st) return st;
+  }
   if (chr_batch_plan(m_max, models[0]->d, lda_max, &cfg) != NAJA_OK) return NAJA_OK;
   DeviceGuard g(models[0]->device);
   int st = chr_batch_occupancy(cfg, ctas_per_sm);

@@ -118,6 +118,7 @@ struct ModelDesc {
   void* samples;     // (nspc * nchains) x d
   double* X_final;   // nullable
   unsigned long long seed;
+  SpArgs sp;         // compressed columns (FP32 tier) for the compressed-column batch
 };
 
 struct BatchConfig {
@@ -126,8 +127,10 @@ struct BatchConfig {
   int slots;        // ring depth, 0 = direct column reads
   int slack_smem;   // 1: slack in shared memory, 0: in registers
   int ctas_per_sm;  // requested resident chains per SM (0 = as many as fit)
-  int lda_max;
+  int lda_max;      // dense: largest padded leading dimension; compressed: largest m
   size_t smem;
+  int sparse;       // 1: the compressed-column kernel (threads 64, 128 or 256)
+  int max_col;      // compressed: entries of the longest column of any model
 };
 
 // Chunk-per-warp capacities instantiated for the batched kernel, per
@@ -145,6 +148,11 @@ inline const int* batch_chunk_capacities(int threads, bool slack_smem) {
 // Validates a batch configuration for models of at most m_max rows and fills
 // rows / smem.  Returns 0 or a naja status code.
 int chr_batch_plan(int m_max, int d, int lda_max, BatchConfig* cfg);
+// The same for the compressed-column kernel (cfg->sparse = 1, cfg->max_col
+// set), with its dispatch.
+int chr_sparse_batch_plan(int m_max, int d, BatchConfig* cfg);
+int chr_sparse_batch_dispatch(const ChrArgs* base, const ModelDesc* models, const int* im, const int* ic, int nitems,
+                              const BatchConfig& cfg, cudaStream_t stream, int* occ_out);
 // Resident CTAs per SM the configuration allows (occupancy calculator).
 int chr_batch_occupancy(const BatchConfig& cfg, int* ctas_per_sm);
 // Persistent launch over nitems (model, chain) work items (device arrays).

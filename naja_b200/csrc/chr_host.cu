@@ -173,6 +173,7 @@ int mrg_init_states(unsigned long long seed, int chain_base, int nchains, void* 
 }
 
 int chr_batch_plan(int m_max, int d, int lda_max, BatchConfig* cfg) {
+  if (cfg->sparse) return chr_sparse_batch_plan(m_max, d, cfg);
   const int nt = cfg->threads;
   if (nt != 128 && nt != 256 && nt != 512) return NAJA_ERR_INVALID_ARGUMENT;
   const int chunks = (m_max + 32 * kBatchV - 1) / (32 * kBatchV), warps = nt / 32;
@@ -196,6 +197,7 @@ int chr_batch_plan(int m_max, int d, int lda_max, BatchConfig* cfg) {
 
 static int batch_dispatch(const ChrArgs* base, const ModelDesc* models, const int* im, const int* ic, int nitems,
                           const BatchConfig& cfg, cudaStream_t stream, int* occ) {
+  if (cfg.sparse) return chr_sparse_batch_dispatch(base, models, im, ic, nitems, cfg, stream, occ);
   switch (cfg.threads) {
     case 128: return chr_batch_dispatch_128(base, models, im, ic, nitems, cfg, stream, occ);
     case 256: return chr_batch_dispatch_256(base, models, im, ic, nitems, cfg, stream, occ);

@@ -450,3 +450,103 @@ int launch_sparse_nw(const ChrArgs& a, const SpArgs& sp, int nchains, const ChrL
 }  // namespace
 }  // namespace chr_detail
 }  // namespace naja
+
+namespace naja {
+namespace chr_detail {
+namespace {
+
+// Batched multi-model run on the compressed-column kernel: the persistent
+// item loop of chr_batched_kernel (one item = one chain of one model; the
+// CTA re-initialises its mbarriers between items, after the producer has
+// drained its copies and every consumer has released its slots), with each
+// model's compressed columns and FP32 tier.  Layout sized for the largest
+// model and the longest column of any model.
+template <int NW>
+__global__ void __launch_bounds__(NW * 32 + 32, NW >= 8 ? 2 : (NW == 4 ? 3 : 4))
+    chr_batched_sparse_kernel(const __grid_constant__ ChrArgs base, const __grid_constant__ Layout L,
+                              const ModelDesc* __restrict__ models, const int* __restrict__ item_model,
+                              const int* __restrict__ item_chain, int nitems) {
+  using Real = float;
+  constexpr int NT = NW * 32;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ ChrArgs item_args;
+  __shared__ SpArgs item_sp;
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);
+  uint64_t* empty = reinterpret_cast<uint64_t*>(smem + L.empty_off);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.flag_off);
+  int* cs = reinterpret_cast<int*>(smem + L.cs_off);
+  if (threadIdx.x == 0) *abort_flag = 0;
+  for (int item = blockIdx.x; item < nitems; item += gridDim.x) {
+    const int ch = item_chain[item];
+    if (threadIdx.x == 0) {
+      for (int s = 0; s < L.slots; ++s) {
+        mbar_init(&full[s], 1);
+        mbar_init(&empty[s], NW);
+      }
+      fence_mbar_init();
+      const ModelDesc& md = models[item_model[item]];
+      ChrArgs a = base;
+      a.A32 = md.A32;
+      a.A64 = md.A64;
+      a.lda = md.lda;
+      a.m = md.m;
+      a.b = md.b;
+      a.X0 = md.X0;
+      a.ldx = md.ldx;
+      a.samples = md.samples;
+      a.X_final = md.X_final;
+      a.seed = md.seed;
+      a.chain_base = 0;
+      a.rng_state = nullptr;
+      a.wait_cycles = nullptr;
+      item_args = a;
+      item_sp = md.sp;
+    }
+    __syncthreads();
+    if (*abort_flag) break;  // every thread reads it after the barrier
+    for (int j = threadIdx.x; j <= item_args.d; j += blockDim.x) cs[j] = item_sp.col_start[j];
+    __syncthreads();
+    if (threadIdx.x >= NT) {
+      if (threadIdx.x == NT)
+        producer_entry<Real, true>(item_args, L, smem, ch, &item_sp, cs, static_cast<int>(sizeof(SpEntry<Real>)));
+    } else {
+      run_sparse_consumers<Real, NW>(item_args, item_sp, L, smem, ch);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int s = 0; s < L.slots; ++s) {
+        mbar_inval(&full[s]);
+        mbar_inval(&empty[s]);
+      }
+    }
+  }
+}
+
+template <int NW>
+int batch_sparse_one(const ChrArgs* base, const ModelDesc* models, const int* im, const int* ic, int nitems,
+                     const BatchConfig& cfg, cudaStream_t stream, int* occ_out) {
+  auto kern = chr_batched_sparse_kernel<NW>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(cfg.smem));
+  if (e != cudaSuccess) return NAJA_ERR_CUDA;
+  int occ = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NW * 32 + 32, cfg.smem);
+  if (e != cudaSuccess) return NAJA_ERR_CUDA;
+  if (occ_out) {
+    *occ_out = occ;
+    return NAJA_OK;
+  }
+  if (occ < 1) return NAJA_ERR_UNSUPPORTED;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int per_sm = cfg.ctas_per_sm > 0 ? (cfg.ctas_per_sm < occ ? cfg.ctas_per_sm : occ) : occ;
+  const int grid = nitems < sms * per_sm ? nitems : sms * per_sm;
+  const Layout L = make_sparse_layout(base->d, cfg.lda_max, sizeof(float), sizeof(SpEntry<float>), cfg.max_col, NW,
+                                      cfg.slots);
+  kern<<<grid, NW * 32 + 32, cfg.smem, stream>>>(*base, L, models, im, ic, nitems);
+  return cudaGetLastError() == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
+}
+
+}  // namespace
+}  // namespace chr_detail
+}  // namespace naja

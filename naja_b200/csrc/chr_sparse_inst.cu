@@ -45,4 +45,28 @@ int chr_sparse_launch(int precision, const ChrArgs& a, const SpArgs& sp, int nch
   if (precision == NAJA_PREC_FP64) return launch_sparse_nw<double>(a, sp, nchains, cfg, stream);
   return launch_sparse_nw<float>(a, sp, nchains, cfg, stream);
 }
+
+int chr_sparse_batch_plan(int m_max, int d, BatchConfig* cfg) {
+  const int nt = cfg->threads;
+  if (nt != 64 && nt != 128 && nt != 256) return NAJA_ERR_INVALID_ARGUMENT;
+  if (cfg->slots < 3 || cfg->slots > kMaxSlots) return NAJA_ERR_INVALID_ARGUMENT;
+  if (cfg->max_col <= 0) return NAJA_ERR_UNSUPPORTED;
+  const Layout L = make_sparse_layout(d, m_max, 4, kSpEntryBytes32, cfg->max_col, nt / 32, cfg->slots);
+  // the kernel also holds one ChrArgs and one SpArgs in static shared memory
+  if (L.total + align_up(sizeof(ChrArgs) + sizeof(SpArgs), 128) > kSmemBudget) return NAJA_ERR_UNSUPPORTED;
+  cfg->rows = 0;
+  cfg->lda_max = m_max;
+  cfg->smem = L.total;
+  return NAJA_OK;
+}
+
+int chr_sparse_batch_dispatch(const ChrArgs* base, const ModelDesc* models, const int* im, const int* ic, int nitems,
+                              const BatchConfig& cfg, cudaStream_t stream, int* occ_out) {
+  switch (cfg.threads) {
+    case 64: return batch_sparse_one<2>(base, models, im, ic, nitems, cfg, stream, occ_out);
+    case 128: return batch_sparse_one<4>(base, models, im, ic, nitems, cfg, stream, occ_out);
+    case 256: return batch_sparse_one<8>(base, models, im, ic, nitems, cfg, stream, occ_out);
+    default: return NAJA_ERR_UNSUPPORTED;
+  }
+}
 }  // namespace naja

@@ -1,6 +1,7 @@
 """Batched multi-model kernel (GPU): every model of a batch reproduces its
-standalone naja_chr_run bit for bit, for every launch shape; a captured
-CUDA graph replays the same result."""
+standalone naja_chr_run bit for bit, for every launch shape of the dense and
+the compressed-column batch kernels; a captured CUDA graph replays the same
+result."""
 import numpy as np
 import pytest
 
@@ -19,7 +20,9 @@ def _models(nmodels=5, n=260, d=70):
 
 
 SHAPES = [Shape(256, 3, 1, 0), Shape(128, 2, 1, 2), Shape(512, 0, 1, 1), Shape(256, 4, 0, 1), Shape(512, 8, 0, 0),
-          Shape(128, 0, 1, 3)]
+          Shape(128, 0, 1, 3),
+          # compressed-column kernel
+          Shape(64, 3, 1, 0, sparse=1), Shape(128, 4, 1, 2, sparse=1), Shape(256, 8, 1, 0, sparse=1)]
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=str)
@@ -57,7 +60,7 @@ def test_graph_replay(cuda):
     direct = [o.clone() for o in outs]
     for o in outs:
         o.zero_()
-    g = B.capture(X, outs, nspc, thin, nch, shape=Shape(256, 3, 1, 0), seed=3, pair_prob=0.3)
+    g = B.capture(X, outs, nspc, thin, nch, shape=Shape(128, 4, 1, 0, sparse=1), seed=3, pair_prob=0.3)
     for _ in range(2):
         g.launch()
     g.check()
