@@ -423,7 +423,7 @@ def _batched(a, torch, dev):
     return {"workload": f"{len(polys)} conditioned variants (m {min(ms_rows)}-{max(ms_rows)}) x {nch} chains x "
                         f"{nspc} samples, thinning {thin}, pair-prob {a.pair_prob}, one persistent launch in a CUDA graph",
             "shape": {"threads": shape.threads, "slots": shape.slots, "slack_smem": shape.slack_smem,
-                      "ctas_per_sm": shape.ctas_per_sm},
+                      "ctas_per_sm": shape.ctas_per_sm, "sparse": shape.sparse},
             "ms": ms, "chr_steps_per_s": steps / (ms / 1e3),
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "peak_source": src, "bytes_per_chr_step": bytes_total / steps},
