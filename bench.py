@@ -348,9 +348,9 @@ def _ours(a, rank, world):
 
 def _e2e(a, W, torch, dev, min_ess):
     import naja_b200 as nb
+    from naja_b200.pipeline import sample_backmapped
 
     pinned_out = torch.empty((W.nspc * W.nchains, W.n), dtype=torch.float32, pin_memory=True)
-    samples = torch.empty((W.nspc * W.nchains, W.d), dtype=torch.float32, device=dev)
     x0 = np.ascontiguousarray(np.broadcast_to(W.start, (W.nchains, W.d)))
     h2d = W.A.nbytes + W.b.nbytes + x0.nbytes + W.T.nbytes + W.shift.nbytes
     d2h = pinned_out.numel() * 4
@@ -360,9 +360,10 @@ def _e2e(a, W, torch, dev, min_ess):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         P = nb.Polytope(W.A, W.b, device=dev.index)
-        P.run(x0, W.nspc, W.thin, W.nchains, out=samples, seed=a.seed, pair_prob=W.pair,
-              resync_interval=a.resync, precision=a.precision, sparse=a.sparse, tpb=a.tpb, stream=None)
-        nb.backmap(W.T, W.shift, samples, mode=a.backmap_mode, out=pinned_out)
+        # sampling, backmap and copy to host overlapped chunk by chunk (same samples as one launch)
+        sample_backmapped(P, W.T, W.shift, x0, W.nspc, W.thin, W.nchains, pinned_out, mode=a.backmap_mode,
+                          seed=a.seed, pair_prob=W.pair, resync_interval=a.resync, precision=a.precision,
+                          sparse=a.sparse, tpb=a.tpb)
         e1.record()
         torch.cuda.synchronize()
         P.close()
