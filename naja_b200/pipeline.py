@@ -55,10 +55,11 @@ def sample_backmapped(P: Polytope, T, shift, X0, nspc: int, thinning: int, nchai
         raise ValueError("sample_backmapped runs whole jobs: no step_offset, chain_base or out_nchains")
     dev = torch.device("cuda", P.device)
     d = P.d
-    T_dev = torch.as_tensor(np.asarray(T, dtype=np.float64) if not torch.is_tensor(T) else T,
-                            dtype=torch.float64).to(dev)
-    sh_dev = torch.as_tensor(np.asarray(shift, dtype=np.float64) if not torch.is_tensor(shift) else shift,
-                             dtype=torch.float64).to(dev)
+    def on_device(v):
+        t = v if torch.is_tensor(v) else torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64))
+        return t.to(device=dev, dtype=torch.float64)
+
+    T_dev, sh_dev = on_device(T), on_device(shift)
     n = T_dev.shape[0]
     if tuple(out.shape) != (nspc * nchains, n):
         raise ValueError(f"out must be ({nspc * nchains}, {n})")
