@@ -55,6 +55,7 @@ def sample_backmapped(P: Polytope, T, shift, X0, nspc: int, thinning: int, nchai
         raise ValueError("sample_backmapped runs whole jobs: no step_offset, chain_base or out_nchains")
     dev = torch.device("cuda", P.device)
     d = P.d
+
     def on_device(v):
         t = v if torch.is_tensor(v) else torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64))
         return t.to(device=dev, dtype=torch.float64)
