@@ -201,6 +201,11 @@ def _backmap_roofline(W, ms, mode):
             "note": "algorithmic FLOPs 2 n d N; the three split products are not credited"}
 
 
+def _stats(v):
+    """min / median / max of per-step times (the per-step lists go to --detail-file)."""
+    return {"min": float(min(v)), "median": float(statistics.median(v)), "max": float(max(v)), "n": len(v)}
+
+
 def _cpu_baseline(W, a, min_ess_per_step):
     import oracle.oracle as O
 
@@ -325,7 +330,8 @@ def _ours(a, rank, world):
                                          "two per pair step, plus the amortised sample write",
                      "compressed_bytes_per_chr_step": W.compressed_bytes_per_step,
                      "chr_steps_per_launch": W.steps},
-        "chr_steps_per_s": steps_per_s, "min_ess": min_ess, "job_ms": job_ms, "chr_ms": chr_ms,
+        "chr_steps_per_s": steps_per_s, "min_ess": min_ess,
+        "job_ms": _stats(job_ms), "chr_ms": _stats(chr_ms),
         "gate": gate,
         "backmap": {"mode": a.backmap_mode, "ms": statistics.mean(bm_ms), "error_vs_fp64": bm_err,
                     "roofline": _backmap_roofline(W, statistics.mean(bm_ms), a.backmap_mode)},
@@ -334,6 +340,11 @@ def _ours(a, rank, world):
         "gpu_launches": a.steps * (1 + (1 if a.backmap_mode == "fp64" else 3)),
     }
     line["clocks"] = clk.summary()
+    detail = {"job_ms": job_ms, "chr_ms": chr_ms, "backmap_ms": bm_ms}
+    if rank == 0 and a.fp64_figure:
+        line["fp64_tier"] = _fp64_figure(a, W, P, x0, torch, dev)
+    if rank == 0 and a.cube:
+        line["unit_cube"] = _unit_cube(a, torch, dev)
     if a.e2e and rank == 0:
         line["e2e"] = _e2e(a, W, torch, dev, min_ess)
     if rank == 0 and world == 1 and not a.no_cpu:
@@ -341,7 +352,10 @@ def _ours(a, rank, world):
     if rank == 0 and a.batch_models > 0:
         line["batched"] = _batched(a, torch, dev)
     if rank == 0 and a.learned_train > 0:
-        line["learned_rounding"] = _learned(a)
+        line["learned_rounding"], detail["learned_rounding"] = _learned(a)
+    if rank == 0 and a.detail_file:
+        Path(a.detail_file).parent.mkdir(parents=True, exist_ok=True)
+        Path(a.detail_file).write_text(json.dumps(detail))
     P.close()
     return line
 
@@ -515,9 +529,88 @@ def _learned(a):
     sampling + rounding-map time."""
     from naja_b200 import learned
 
-    return learned.run_experiment(n=a.n, d=a.d, n_train=a.learned_train, n_test=a.learned_test,
+    full = learned.run_experiment(n=a.n, d=a.d, n_train=a.learned_train, n_test=a.learned_test,
                                   nchains=8, nspc_train=500, nspc_test=1000, thinning=a.thinning,
                                   pair_prob=a.pair_prob, epochs=a.learned_epochs, resync=a.resync, seed=a.seed)
+    return _strip_lists(full), full
+
+
+def _strip_lists(obj):
+    """The same record without lists longer than 8 values (kept in --detail-file)."""
+    if isinstance(obj, dict):
+        return {k: _strip_lists(v) for k, v in obj.items() if not (isinstance(v, list) and len(v) > 8)}
+    return obj
+
+
+def _fp64_figure(a, W, P, x0, torch, dev):
+    """The same job in the FP64 tier (the reference's arithmetic): FP64 A,
+    slack, ratios and alpha, samples written as float.  Two timed jobs after
+    one warm-up; min-ESS/s of the last job, sampling + backmap time."""
+    from naja_b200 import backmap
+    from naja_b200 import validate as nv
+
+    samples = torch.empty((W.nspc * W.nchains, W.d), dtype=torch.float32, device=dev)
+    V = torch.empty((W.nspc * W.nchains, W.n), dtype=torch.float32, device=dev)
+    T_dev = torch.from_numpy(W.T).to(dev)
+    sh_dev = torch.from_numpy(W.shift).to(dev)
+    times = []
+    for k in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        P.run(x0, W.nspc, W.thin, W.nchains, out=samples, seed=a.seed, pair_prob=W.pair, resync_interval=0,
+              precision="fp64", sparse=a.sparse)
+        backmap(T_dev, sh_dev, samples, mode=a.backmap_mode, out=V)
+        e1.record()
+        torch.cuda.synchronize()
+        if k:
+            times.append(e0.elapsed_time(e1))
+    P.check()
+    ess, rhat = nv.ess_rhat(samples, W.nchains, layout=1)
+    ms = statistics.mean(times)
+    min_ess = float(ess.sum(axis=1).min())
+    choice = P.kernel_choice(W.nspc, W.thin, W.nchains, pair_prob=W.pair, precision="fp64", sparse=a.sparse)
+    return {"value": min_ess / (ms / 1e3), "unit": UNIT, "ms_per_job": ms, "min_ess": min_ess,
+            "rhat_max": float(rhat.max()), "chr_steps_per_s": W.steps / (ms / 1e3),
+            "kernel": choice["kernel"], "threads": choice["threads"],
+            "note": "FP64 tier (no FP32 slack, no recompute needed), same workload and streams"}
+
+
+def _unit_cube(a, torch, dev):
+    """The unit-cube workload [0,1]^50 (A = [I; -I], b = [1; 0], start at the
+    centre), 4 chains x 2000 samples, thinning 8, pair-prob 0, Philox seed 0,
+    FP32 tier: chain-steps/s, the largest deviation of a coordinate's mean
+    from 1/2 and variance from 1/12 in units of its standard error at the
+    measured ESS, split-R-hat and min-ESS/s."""
+    from naja_b200 import Polytope, synth
+    from naja_b200 import validate as nv
+
+    A, b, x0 = synth.unit_cube_stacked(50)
+    P = Polytope(A, b, device=dev.index)
+    nspc, thin, nch = 2000, 8, 4
+    out = torch.empty((nspc * nch, 50), dtype=torch.float32, device=dev)
+    times = []
+    for k in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        P.run(x0, nspc, thin, nch, out=out, seed=0, pair_prob=0.0, precision="fp32")
+        e1.record()
+        torch.cuda.synchronize()
+        if k:
+            times.append(e0.elapsed_time(e1))
+    P.check()
+    ess, rhat = nv.ess_rhat(out, nch, layout=1)
+    per_dim = ess.sum(axis=1)
+    y = out.double().cpu().numpy()
+    z_mean = np.abs(y.mean(axis=0) - 0.5) / np.sqrt((1 / 12) / per_dim)
+    z_var = np.abs(y.var(axis=0, ddof=1) - 1 / 12) / np.sqrt((1 / 80 - 1 / 144) / per_dim)
+    ms = statistics.mean(times)
+    choice = P.kernel_choice(nspc, thin, nch)
+    P.close()
+    return {"workload": "unit cube [0,1]^50, 4 chains x 2000 samples, thinning 8, pair-prob 0, seed 0",
+            "ms": ms, "chr_steps_per_s": nch * nspc * thin / (ms / 1e3), "kernel": choice["kernel"],
+            "mean_max_dev_in_se": float(z_mean.max()), "var_max_dev_in_se": float(z_var.max()),
+            "rhat_max": float(rhat.max()), "min_ess": float(per_dim.min()),
+            "min_ess_per_s": float(per_dim.min()) / (ms / 1e3)}
 
 
 def _reference_arm(a, rank, world):
@@ -529,27 +622,21 @@ def _reference_arm(a, rank, world):
     (CoordinateHitAndRun, then backmap_into as CoordinateHitAndRunBackmap
     does) with the reference's defaults: FP64, cuRAND MRG32k3a, 128 threads
     per chain.  Time = the call plus cudaDeviceSynchronize, as
-    src/engine/job_sampling.cu measures sampling.  Each step is a bounded
-    sample of the workload (fewer samples per chain, same chains, polytope,
-    thinning and pair-prob); its min-ESS comes from the CPU oracle's ESS on
-    the reference's own samples.  Without the reference build the CPU
-    restatement of the same algorithm (oracle/) is timed instead.
+    src/engine/job_sampling.cu measures sampling.  Every timed step is the
+    whole job (the same chains, samples per chain, polytope, thinning,
+    pair-prob and backmap as this project's arm); its min-ESS comes from the
+    ESS estimator (FFT autocovariance, FP64) on the reference's own samples.
+    Without the reference build the CPU restatement of the same algorithm
+    (oracle/) is timed instead, on a bounded sample of the workload.
     """
     import oracle.oracle as O
 
     W = Workload(a)
     if O.reference_available() and not a.ref_cpu:
         cal_nspc = 20
-        # two calibration runs separate the per-call setup from the per-sample time
-        _, _, ms_a = O.reference_chr_run(W.A, W.b, W.start, cal_nspc, W.thin, W.nchains, tpb=128, seed=a.seed,
-                                         pair_prob=W.pair, T=W.T, shift=W.shift, want_samples=False)
-        _, _, ms_b = O.reference_chr_run(W.A, W.b, W.start, 10 * cal_nspc, W.thin, W.nchains, tpb=128,
-                                         seed=a.seed, pair_prob=W.pair, T=W.T, shift=W.shift, want_samples=False)
-        per_sample_ms = max(1e-6, (ms_b - ms_a) / (9 * cal_nspc))
-        # The full workload per timed step unless K steps would exceed the time
-        # budget; warm-up steps are short runs (they only warm the context,
-        # module loading and cuBLAS).
-        nspc = int(max(50, min(W.nspc, a.ref_budget_s * 1e3 / (a.steps * per_sample_ms))))
+        # The full workload in every timed step; warm-up steps are short runs
+        # (they only warm the context, module loading and cuBLAS).
+        nspc = W.nspc
         times = []
         S = None
         for k in range(a.warmup + a.steps):
@@ -564,9 +651,9 @@ def _reference_arm(a, rank, world):
                 S = S_k
         kind, cores = "reference", 0
         sample = (f"reference CoordinateHitAndRun + backmap_into (FP64, cuRAND MRG32k3a, 128 threads/chain) "
-                  f"compiled from its sources for sm_100a: {W.nchains} chains x {nspc} samples (thinning {W.thin}) "
-                  f"of the {W.nspc}-sample workload per timed step; warm-up steps {cal_nspc} samples; min-ESS "
-                  f"from its own samples")
+                  f"compiled from its sources for sm_100a: the full workload ({W.nchains} chains x {nspc} samples, "
+                  f"thinning {W.thin}, backmap to n={W.n}) in every timed step; warm-up steps {cal_nspc} samples; "
+                  f"min-ESS from its own samples of the last step")
         dtype = "f64"
     else:
         cores = os.cpu_count() or 1
@@ -628,14 +715,17 @@ def main(argv=None):
     ap.add_argument("--batch-chains", type=int, default=8)
     ap.add_argument("--batch-nspc", type=int, default=4000)
     ap.add_argument("--batch-shape", default="", help="threads,slots,slack_smem,ctas_per_sm[,sparse] (skips the autotuner)")
-    ap.add_argument("--ref-budget-s", type=float, default=200.0,
-                    help="reference arm: time budget of the K timed steps")
     ap.add_argument("--ref-cpu", action="store_true", help="reference arm: time the CPU restatement")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--learned-train", type=int, default=256,
                     help="learned-rounding section: training variants (0 = skip)")
     ap.add_argument("--learned-test", type=int, default=16)
     ap.add_argument("--learned-epochs", type=int, default=60)
+    ap.add_argument("--no-fp64-figure", dest="fp64_figure", action="store_false",
+                    help="skip the FP64-tier figure of the same job")
+    ap.add_argument("--no-cube", dest="cube", action="store_false", help="skip the unit-cube workload")
+    ap.add_argument("--detail-file", default="",
+                    help="write per-step times and per-variant records here (JSON)")
     ap.add_argument("--precision-study", action="store_true",
                     help="run only the FP32/FP64 tier and backmap precision study and print it")
     a = ap.parse_args(argv)

@@ -266,15 +266,17 @@ inline DMatrix<double> CoordinateHitAndRunBackmap(
     throw std::invalid_argument("backmap_into: transformation shape mismatch with samples");
   if (shift_d.len != transformation_d.rows)
     throw std::invalid_argument("backmap_into: shift length mismatch with transformation rows");
-  DMatrix<double> Y = CoordinateHitAndRun(A_d, b_d, X_d, nspc, thinning, nchains, tpb_ss, seed, pair_prob,
-                                          resync_interval, ksparse_prob, ksparse_k, pair_mode, pair_i, pair_j, pair_c,
-                                          pair_s, tier);
-  DMatrix<double> V(transformation_d.rows, Y.cols);
-  detail::throw_status(naja_backmap(transformation_d.rows, transformation_d.cols, Y.cols, transformation_d.dmat,
-                                    transformation_d.rows, shift_d.dvec, Y.dmat, NAJA_DTYPE_F64, V.dmat,
-                                    NAJA_DTYPE_F64, backmap_mode, nullptr),
-                       "backmap_into");
-  detail::cuda_check(cudaDeviceSynchronize(), "backmap_into");
+  // One library call: sampling, then the backmap of each chunk of samples
+  // while the next chunk samples (a single chunk for the MRG32k3a streams or
+  // without a resync interval); the samples are those of CoordinateHitAndRun.
+  detail::PolytopeHandle P(A_d, b_d);
+  naja_chr_params p = detail::make_params(nspc, thinning, nchains, tpb_ss, seed, pair_prob, resync_interval,
+                                          ksparse_prob, ksparse_k, pair_mode, pair_i, pair_j, pair_c, pair_s, tier);
+  DMatrix<double> V(transformation_d.rows, nchains * nspc);
+  detail::throw_status(naja_chr_run_backmapped(P.p, &p, X_d.dmat, X_d.rows, transformation_d.rows,
+                                               transformation_d.dmat, transformation_d.rows, shift_d.dvec,
+                                               backmap_mode, V.dmat, NAJA_DTYPE_F64, nullptr, nullptr, 0, nullptr),
+                       "CoordinateHitAndRunBackmap");
   return V;
 }
 

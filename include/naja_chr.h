@@ -5,7 +5,9 @@
  * Plain C: pointers, sizes, POD structs, an integer status and a
  * thread-local last-error string.  Every pointer argument may be host or
  * device memory (the library inspects it); device pointers must live on the
- * device the call runs on.  Calls are asynchronous on the given stream
+ * device the call runs on (device memory of another GPU is rejected with
+ * NAJA_ERR_INVALID_ARGUMENT; managed memory is accepted).  Calls are
+ * asynchronous on the given stream
  * unless a host pointer forces a synchronous copy back.  Matrices are
  * column-major with an explicit leading dimension, as in the reference
  * (IDX2C(i,j,ld) = j*ld + i, src/gpu/helper.h:9 of quothbonney/naja).
@@ -193,12 +195,37 @@ int naja_backmap(int n, int d, long long N, const double* T, int ldt, const doub
  * process exit; a call needing more (about 1 KiB + 2 * N * dp * e +
  * 2 * n * dp * e bytes, dp = d rounded up to 64, e = 2 for BF16X3 and 4
  * for TF32X3) is rejected with NAJA_ERR_INVALID_ARGUMENT: split N across
- * calls.  The first call on a device looks the array up on that device;
- * make it before any stream capture.  Calls share the array: calls whose
- * work overlaps on the GPU race.  Synchronises `stream` to read its error
- * word. */
+ * calls.  The first call on a device does the set-up: it looks the array's
+ * device address up with that device current and caches it; make that first
+ * call before any stream capture, and do not call this entry point again on
+ * a device after cudaDeviceReset of it.  All calls on a device share the
+ * array: calls whose work overlaps on the GPU (other streams, other host
+ * threads) race, so the caller serialises them.  Synchronises `stream` to
+ * read its error word. */
 int naja_backmap_noalloc(int n, int d, long long N, const double* T, int ldt, const double* shift,
                          const void* Y, int y_dtype, void* V, int v_dtype, int mode, void* stream);
+
+/* ------------------------------------------------------------ pipeline */
+
+/* naja_chr_run followed by naja_backmap as one job, overlapped: the chains
+ * run in chunks of chunk_nspc samples (<= 0: automatic, whole
+ * lcm(resync_interval, thinning) periods of about 65,536 steps) on one
+ * stream while the previous chunk's backmap V = T y + shift and the copies of
+ * its rows run on another.  V receives nspc*nchains rows of n values
+ * (v_dtype) in the sample order of naja_chr_run; `samples` (nullable) also
+ * receives the samples themselves (params->out_dtype).  V, samples, X0,
+ * X_final, T and shift may be host or device memory; pinned host memory
+ * lets the copies overlap the sampling.  Chunking needs the Philox streams
+ * and resync_interval > 0 (a chunk starts where one run recomputes the slack
+ * anyway, so the samples are those of one naja_chr_run, bit for bit);
+ * otherwise the job runs as one chunk.  chain_base must be 0 and out_nchains
+ * 0 or nchains.  Synchronises `stream` and reports device-side errors before
+ * returning.  Replaces the sample-then-backmap-then-copy sequence of
+ * run_sampling_job (src/engine/job_sampling.cu:300-385) around
+ * CoordinateHitAndRunBackmap (src/gpu/chr.cu:72-99). */
+int naja_chr_run_backmapped(const naja_polytope* P, const naja_chr_params* params, const double* X0, int ldx,
+                            int n, const double* T, int ldt, const double* shift, int mode, void* V, int v_dtype,
+                            void* samples, double* X_final, int chunk_nspc, void* stream);
 
 /* ------------------------------------------------------------ validate */
 

@@ -55,6 +55,7 @@ EXPORTED = (
     "naja_graph_launch",
     "naja_graph_check",
     "naja_graph_destroy",
+    "naja_chr_run_backmapped",
 )
 
 # Every entry point include/naja_mlp.h declares.
@@ -178,6 +179,7 @@ def load() -> C.CDLL:
     lib.naja_graph_launch.argtypes = [vp, vp]
     lib.naja_graph_check.argtypes = [vp]
     lib.naja_graph_destroy.argtypes = [vp]
+    lib.naja_chr_run_backmapped.argtypes = [vp, C.POINTER(ChrParams), vp, i, i, vp, i, vp, i, vp, i, vp, vp, i, vp]
     f = C.c_float
     lib.naja_gemm_bf16.argtypes = [i, i, i, vp, i, vp, i, C.POINTER(GemmEpilogue), vp]
     lib.naja_mlp_check.argtypes = [vp]
@@ -195,7 +197,7 @@ def load() -> C.CDLL:
                                                "naja_validate", "naja_mrg_tape", "naja_mrg_init_states",
                                                "naja_chr_run_batched", "naja_batch_occupancy",
                                                "naja_chr_capture_batched", "naja_graph_launch", "naja_graph_check",
-                                               "naja_graph_destroy"):
+                                               "naja_graph_destroy", "naja_chr_run_backmapped"):
             f.restype = C.c_int
     _lib = lib
     return lib

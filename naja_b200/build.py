@@ -41,6 +41,7 @@ def _units():
     units.append(("chr_sparse", CSRC / "chr_sparse_inst.cu", ["-fmad=false"]))
     units.append(("chr_host", CSRC / "chr_host.cu", ["-fmad=false"]))
     units.append(("capi", CSRC / "capi.cu", []))
+    units.append(("pipeline", CSRC / "pipeline.cu", []))
     units.append(("validate", CSRC / "validate.cu", ["-fmad=false"]))
     units.append(("backmap", CSRC / "backmap.cu", ["-fmad=false"]))
     units.append(("backmap_tc", CSRC / "backmap_tc.cu", []))

@@ -518,13 +518,6 @@ int run_sampling(const RunConfig& c) {
   p.rng = c.rng == "mrg" ? NAJA_RNG_REF_MRG : NAJA_RNG_PHILOX;
   p.out_dtype = NAJA_DTYPE_F32;
   const long long N = static_cast<long long>(c.n_samples) * c.n_chains;
-  std::vector<float> Y(static_cast<size_t>(N) * d);
-  phase(st, c.backmap ? "gpu sampling+backmap" : "gpu sampling");
-  t0 = std::chrono::steady_clock::now();
-  int rc = naja_chr_run(P, &p, X0.data(), d, Y.data(), nullptr, nullptr);
-  prof.sampling = seconds_since(t0);
-  naja_polytope_destroy(P);
-  check(rc);
   std::vector<float> out;
   long long dim = d;
   std::vector<double> Tcm, shift, lb, ub;
@@ -539,13 +532,24 @@ int run_sampling(const RunConfig& c) {
     out.resize(static_cast<size_t>(N) * dim);
     const int mode = c.backmap_mode == "tf32x3" ? NAJA_BACKMAP_TF32X3
                      : c.backmap_mode == "bf16x3" ? NAJA_BACKMAP_BF16X3 : NAJA_BACKMAP_FP64;
+    // Sampling and the backmap of each chunk overlapped in one call; the
+    // reference times the backmap inside the sampling call too
+    // (job_sampling.cu:313-336).
+    phase(st, "gpu sampling+backmap");
     t0 = std::chrono::steady_clock::now();
-    check(naja_backmap(T.rows, d, N, Tcm.data(), T.rows, shift.data(), Y.data(), NAJA_DTYPE_F32, out.data(),
-                       NAJA_DTYPE_F32, mode, nullptr));
-    // the reference times the backmap inside the sampling call (job_sampling.cu:313-336)
-    prof.sampling += seconds_since(t0);
+    int rc = naja_chr_run_backmapped(P, &p, X0.data(), d, T.rows, Tcm.data(), T.rows, shift.data(), mode, out.data(),
+                                     NAJA_DTYPE_F32, nullptr, nullptr, 0, nullptr);
+    prof.sampling = seconds_since(t0);
+    naja_polytope_destroy(P);
+    check(rc);
   } else {
-    out.swap(Y);
+    out.resize(static_cast<size_t>(N) * d);
+    phase(st, "gpu sampling");
+    t0 = std::chrono::steady_clock::now();
+    int rc = naja_chr_run(P, &p, X0.data(), d, out.data(), nullptr, nullptr);
+    prof.sampling = seconds_since(t0);
+    naja_polytope_destroy(P);
+    check(rc);
   }
   prof.throughput = prof.sampling > 0 ? static_cast<double>(N) / prof.sampling : 0.0;
   if (st) std::cout << "> done: " << std::fixed << std::setprecision(1) << prof.sampling << "s, " << std::setprecision(0)

@@ -22,11 +22,6 @@
 
 namespace naja {
 
-int backmap_tc(int n, int d, long long N, const double* T, int ldt, const double* shift, const void* Y, int y_dtype,
-               void* V, int v_dtype, int mode, cudaStream_t stream);
-int backmap_tc_noalloc(int n, int d, long long N, const double* T, int ldt, const double* shift, const void* Y,
-                       int y_dtype, void* V, int v_dtype, int mode, cudaStream_t stream);
-
 namespace {
 
 constexpr int kBM = 64;  // samples per CTA tile
@@ -95,6 +90,20 @@ int launch_fp64(int n, int d, long long N, const double* T, int ldt, const doubl
 }
 
 }  // namespace
+
+int backmap_fp64_enqueue(int n, int d, long long N, const double* T, int ldt, const double* shift, const void* Y,
+                         int y_dtype, void* V, int v_dtype, cudaStream_t stream) {
+  int st;
+  if (y_dtype == NAJA_DTYPE_F32)
+    st = v_dtype == NAJA_DTYPE_F32 ? launch_fp64<float, float>(n, d, N, T, ldt, shift, Y, V, stream)
+                                   : launch_fp64<float, double>(n, d, N, T, ldt, shift, Y, V, stream);
+  else
+    st = v_dtype == NAJA_DTYPE_F32 ? launch_fp64<double, float>(n, d, N, T, ldt, shift, Y, V, stream)
+                                   : launch_fp64<double, double>(n, d, N, T, ldt, shift, Y, V, stream);
+  if (st) return fail(st, std::string("backmap: launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+  return NAJA_OK;
+}
+
 }  // namespace naja
 
 using namespace naja;
@@ -106,6 +115,7 @@ extern "C" int naja_backmap(int n, int d, long long N, const double* T, int ldt,
   if (ldt < n) return fail(NAJA_ERR_INVALID_ARGUMENT, "backmap_into: transformation shape mismatch with samples");
   if ((y_dtype != NAJA_DTYPE_F32 && y_dtype != NAJA_DTYPE_F64) || (v_dtype != NAJA_DTYPE_F32 && v_dtype != NAJA_DTYPE_F64))
     return fail(NAJA_ERR_INVALID_ARGUMENT, "backmap_into: unknown dtype");
+  if (int st = require_local("backmap_into", {T, shift, Y, V})) return st;
   if (N == 0) return NAJA_OK;
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
   const size_t ybytes = static_cast<size_t>(N) * d * (y_dtype == NAJA_DTYPE_F64 ? 8 : 4);
@@ -126,13 +136,7 @@ extern "C" int naja_backmap(int n, int d, long long N, const double* T, int ldt,
   const double* Td = static_cast<const double*>(dT);
   const double* Sd = static_cast<const double*>(dS);
   if (mode == NAJA_BACKMAP_FP64) {
-    if (y_dtype == NAJA_DTYPE_F32)
-      st = v_dtype == NAJA_DTYPE_F32 ? launch_fp64<float, float>(n, d, N, Td, ldt, Sd, dY, dV, stream)
-                                     : launch_fp64<float, double>(n, d, N, Td, ldt, Sd, dY, dV, stream);
-    else
-      st = v_dtype == NAJA_DTYPE_F32 ? launch_fp64<double, float>(n, d, N, Td, ldt, Sd, dY, dV, stream)
-                                     : launch_fp64<double, double>(n, d, N, Td, ldt, Sd, dY, dV, stream);
-    if (st) return fail(st, std::string("backmap: launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+    if ((st = backmap_fp64_enqueue(n, d, N, Td, ldt, Sd, dY, y_dtype, dV, v_dtype, stream))) return st;
   } else if (mode == NAJA_BACKMAP_BF16X3 || mode == NAJA_BACKMAP_TF32X3) {
     st = backmap_tc(n, d, N, Td, ldt, Sd, dY, y_dtype, dV, v_dtype, mode, stream);
     if (st) return st;
@@ -158,6 +162,7 @@ extern "C" int naja_backmap_noalloc(int n, int d, long long N, const double* T, 
   // Host buffers would need staging copies, i.e. allocations: every buffer must be device memory.
   if (!is_device_ptr(T) || !is_device_ptr(shift) || !is_device_ptr(Y) || !is_device_ptr(V))
     return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_backmap_noalloc: T, shift, Y and V must be device memory");
+  if (int st = require_local("naja_backmap_noalloc", {T, shift, Y, V})) return st;
   if (N == 0) return NAJA_OK;
   return backmap_tc_noalloc(n, d, N, T, ldt, shift, Y, y_dtype, V, v_dtype, mode, static_cast<cudaStream_t>(stream_ptr));
 }

@@ -406,35 +406,45 @@ bool make_map(CUtensorMap* m, void* base, bool tf32, long long rows, int dp, int
 
 }  // namespace
 
-int backmap_tc(int n, int d, long long N, const double* T, int ldt, const double* shift, const void* Y, int y_dtype,
-               void* V, int v_dtype, int mode, cudaStream_t stream) {
+size_t backmap_tc_operand_bytes(long long rows, int d, int mode) {
+  const size_t esz = mode == NAJA_BACKMAP_TF32X3 ? 4 : 2;
+  const size_t dp = static_cast<size_t>((d + 63) / 64 * 64);
+  return (static_cast<size_t>(rows) * dp * esz + 1023) / 1024 * 1024;
+}
+
+int backmap_tc_split_T(int n, int d, const double* T, int ldt, void* Th, void* Tl, int mode, cudaStream_t stream) {
+  const int dp = (d + 63) / 64 * 64;
+  const int sblocks = 148 * 8;
+  if (mode == NAJA_BACKMAP_TF32X3)
+    split_T_kernel<true><<<sblocks, 256, 0, stream>>>(T, ldt, n, d, dp, Th, Tl);
+  else
+    split_T_kernel<false><<<sblocks, 256, 0, stream>>>(T, ldt, n, d, dp, Th, Tl);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("backmap: split launch failed: ") + cudaGetErrorString(e));
+  return NAJA_OK;
+}
+
+int backmap_tc_enqueue(int n, int d, long long N, const void* Y, int y_dtype, const void* Th, const void* Tl, void* Yh,
+                       void* Yl, const double* shift, void* V, int v_dtype, int mode, int* err, cudaStream_t stream) {
   const bool tf32 = mode == NAJA_BACKMAP_TF32X3;
   const int esz = tf32 ? 4 : 2;
   const int dp = (d + 63) / 64 * 64;
-  const size_t ybytes = static_cast<size_t>(N) * dp * esz, tbytes = static_cast<size_t>(n) * dp * esz;
-  DeviceBuffer bYh, bYl, bTh, bTl, berr;
-  int st;
-  if ((st = bYh.alloc(ybytes, stream)) || (st = bYl.alloc(ybytes, stream)) || (st = bTh.alloc(tbytes, stream)) ||
-      (st = bTl.alloc(tbytes, stream)) || (st = berr.alloc(4 * sizeof(int), stream)))
-    return st;
-  cudaMemsetAsync(berr.ptr, 0, 4 * sizeof(int), stream);
   const int sblocks = 148 * 8;
   if (tf32) {
     if (y_dtype == NAJA_DTYPE_F64)
-      split_rows_kernel<double, true><<<sblocks, 256, 0, stream>>>(static_cast<const double*>(Y), N, d, dp, bYh.ptr, bYl.ptr);
+      split_rows_kernel<double, true><<<sblocks, 256, 0, stream>>>(static_cast<const double*>(Y), N, d, dp, Yh, Yl);
     else
-      split_rows_kernel<float, true><<<sblocks, 256, 0, stream>>>(static_cast<const float*>(Y), N, d, dp, bYh.ptr, bYl.ptr);
-    split_T_kernel<true><<<sblocks, 256, 0, stream>>>(T, ldt, n, d, dp, bTh.ptr, bTl.ptr);
+      split_rows_kernel<float, true><<<sblocks, 256, 0, stream>>>(static_cast<const float*>(Y), N, d, dp, Yh, Yl);
   } else {
     if (y_dtype == NAJA_DTYPE_F64)
-      split_rows_kernel<double, false><<<sblocks, 256, 0, stream>>>(static_cast<const double*>(Y), N, d, dp, bYh.ptr, bYl.ptr);
+      split_rows_kernel<double, false><<<sblocks, 256, 0, stream>>>(static_cast<const double*>(Y), N, d, dp, Yh, Yl);
     else
-      split_rows_kernel<float, false><<<sblocks, 256, 0, stream>>>(static_cast<const float*>(Y), N, d, dp, bYh.ptr, bYl.ptr);
-    split_T_kernel<false><<<sblocks, 256, 0, stream>>>(T, ldt, n, d, dp, bTh.ptr, bTl.ptr);
+      split_rows_kernel<float, false><<<sblocks, 256, 0, stream>>>(static_cast<const float*>(Y), N, d, dp, Yh, Yl);
   }
   CUtensorMap mAh, mAl, mBh, mBl;
-  if (!make_map(&mAh, bYh.ptr, tf32, N, dp, kTileM) || !make_map(&mAl, bYl.ptr, tf32, N, dp, kTileM) ||
-      !make_map(&mBh, bTh.ptr, tf32, n, dp, kTileN) || !make_map(&mBl, bTl.ptr, tf32, n, dp, kTileN))
+  if (!make_map(&mAh, Yh, tf32, N, dp, kTileM) || !make_map(&mAl, Yl, tf32, N, dp, kTileM) ||
+      !make_map(&mBh, const_cast<void*>(Th), tf32, n, dp, kTileN) ||
+      !make_map(&mBl, const_cast<void*>(Tl), tf32, n, dp, kTileN))
     return fail(NAJA_ERR_CUDA, "backmap: cuTensorMapEncodeTiled failed");
   TcArgs a;
   a.n = n;
@@ -445,10 +455,9 @@ int backmap_tc(int n, int d, long long N, const double* T, int ldt, const double
   a.shift = shift;
   a.V = V;
   a.v_f64 = v_dtype == NAJA_DTYPE_F64;
-  a.err = static_cast<int*>(berr.ptr);
+  a.err = err;
   const size_t smem = kStages * kStageBytes + 1024 + 256 + 4 * 32 * 33 * sizeof(float);
-  int sms = 148;
-  int dev = 0;
+  int sms = 148, dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = static_cast<int>(std::min<long long>(sms, a.tiles));
@@ -458,15 +467,37 @@ int backmap_tc(int n, int d, long long N, const double* T, int ldt, const double
   kern<<<grid, kThreads, smem, stream>>>(mAh, mAl, mBh, mBl, a);
   e = cudaGetLastError();
   if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("backmap: launch failed: ") + cudaGetErrorString(e));
-  int w[4] = {0, 0, 0, 0};
-  e = cudaMemcpyAsync(w, berr.ptr, sizeof(w), cudaMemcpyDeviceToHost, stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("backmap: ") + cudaGetErrorString(e));
-  if (w[0] != 0)
-    return fail(NAJA_ERR_DEVICE, "backmap: tensor-core pipeline gave up a bounded wait (code " + std::to_string(w[0]) +
-                                     ", " + std::to_string(w[1]) + ", " + std::to_string(w[2]) + ", " +
-                                     std::to_string(w[3]) + ")");
   return NAJA_OK;
+}
+
+int backmap_tc_read_error(const int* err, cudaStream_t stream, const char* who) {
+  int w[4] = {0, 0, 0, 0};
+  cudaError_t e = cudaMemcpyAsync(w, err, sizeof(w), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string(who) + ": " + cudaGetErrorString(e));
+  if (w[0] != 0)
+    return fail(NAJA_ERR_DEVICE, std::string(who) + ": tensor-core pipeline gave up a bounded wait (code " +
+                                     std::to_string(w[0]) + ", " + std::to_string(w[1]) + ", " + std::to_string(w[2]) +
+                                     ", " + std::to_string(w[3]) + ")");
+  return NAJA_OK;
+}
+
+int backmap_tc(int n, int d, long long N, const double* T, int ldt, const double* shift, const void* Y, int y_dtype,
+               void* V, int v_dtype, int mode, cudaStream_t stream) {
+  const size_t ybytes = backmap_tc_operand_bytes(N, d, mode), tbytes = backmap_tc_operand_bytes(n, d, mode);
+  DeviceBuffer bYh, bYl, bTh, bTl, berr;
+  int st;
+  if ((st = bYh.alloc(ybytes, stream)) || (st = bYl.alloc(ybytes, stream)) || (st = bTh.alloc(tbytes, stream)) ||
+      (st = bTl.alloc(tbytes, stream)) || (st = berr.alloc(4 * sizeof(int), stream)))
+    return st;
+  int* err = static_cast<int*>(berr.ptr);
+  cudaError_t e = cudaMemsetAsync(err, 0, 4 * sizeof(int), stream);
+  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("backmap: ") + cudaGetErrorString(e));
+  if ((st = backmap_tc_split_T(n, d, T, ldt, bTh.ptr, bTl.ptr, mode, stream))) return st;
+  if ((st = backmap_tc_enqueue(n, d, N, Y, y_dtype, bTh.ptr, bTl.ptr, bYh.ptr, bYl.ptr, shift, V, v_dtype, mode, err,
+                               stream)))
+    return st;
+  return backmap_tc_read_error(err, stream, "backmap");
 }
 
 // ----------------------------------------------------------------------
@@ -482,9 +513,12 @@ int backmap_tc(int n, int d, long long N, const double* T, int ldt, const double
 // held until the process exits.  Its device address is looked up once per
 // device (cudaGetSymbolAddress, with that device current) on the first call
 // made on that device; that first call should therefore come before any
-// stream capture.  Every call reuses the same array: the error words are
-// cleared by each call, and calls whose work overlaps on the GPU (different
-// streams, or different host threads on one device) race on the array.
+// stream capture.  After cudaDeviceReset the cached address is stale: a
+// process that resets a device must not call this entry point on it again.
+// Every call reuses the same array: the error words are cleared by each call,
+// and calls whose work overlaps on the GPU (different streams, or different
+// host threads on one device) race on the array, so the caller serialises
+// them.
 constexpr size_t kNoAllocScratchBytes = 64ull << 20;  // 64 MiB
 constexpr int kNoAllocMaxDevices = 64;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -513,12 +547,8 @@ int noalloc_scratch(unsigned char** out) {
 
 int backmap_tc_noalloc(int n, int d, long long N, const double* T, int ldt, const double* shift, const void* Y,
                        int y_dtype, void* V, int v_dtype, int mode, cudaStream_t stream) {
-  const bool tf32 = mode == NAJA_BACKMAP_TF32X3;
-  const int esz = tf32 ? 4 : 2;
-  const int dp = (d + 63) / 64 * 64;
   // scratch layout: [error words | Y hi | Y lo | T hi | T lo], each 1024-aligned
-  auto up = [](size_t v) { return (v + 1023) / 1024 * 1024; };
-  const size_t ybytes = up(static_cast<size_t>(N) * dp * esz), tbytes = up(static_cast<size_t>(n) * dp * esz);
+  const size_t ybytes = backmap_tc_operand_bytes(N, d, mode), tbytes = backmap_tc_operand_bytes(n, d, mode);
   const size_t need = 1024 + 2 * ybytes + 2 * tbytes;
   if (need > kNoAllocScratchBytes)
     return fail(NAJA_ERR_INVALID_ARGUMENT,
@@ -534,54 +564,9 @@ int backmap_tc_noalloc(int n, int d, long long N, const double* T, int ldt, cons
   void* Tl = base + 1024 + 2 * ybytes + tbytes;
   cudaError_t e = cudaMemsetAsync(err, 0, 4 * sizeof(int), stream);
   if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_backmap_noalloc: ") + cudaGetErrorString(e));
-  const int sblocks = 148 * 8;
-  if (tf32) {
-    if (y_dtype == NAJA_DTYPE_F64)
-      split_rows_kernel<double, true><<<sblocks, 256, 0, stream>>>(static_cast<const double*>(Y), N, d, dp, Yh, Yl);
-    else
-      split_rows_kernel<float, true><<<sblocks, 256, 0, stream>>>(static_cast<const float*>(Y), N, d, dp, Yh, Yl);
-    split_T_kernel<true><<<sblocks, 256, 0, stream>>>(T, ldt, n, d, dp, Th, Tl);
-  } else {
-    if (y_dtype == NAJA_DTYPE_F64)
-      split_rows_kernel<double, false><<<sblocks, 256, 0, stream>>>(static_cast<const double*>(Y), N, d, dp, Yh, Yl);
-    else
-      split_rows_kernel<float, false><<<sblocks, 256, 0, stream>>>(static_cast<const float*>(Y), N, d, dp, Yh, Yl);
-    split_T_kernel<false><<<sblocks, 256, 0, stream>>>(T, ldt, n, d, dp, Th, Tl);
-  }
-  CUtensorMap mAh, mAl, mBh, mBl;
-  if (!make_map(&mAh, Yh, tf32, N, dp, kTileM) || !make_map(&mAl, Yl, tf32, N, dp, kTileM) ||
-      !make_map(&mBh, Th, tf32, n, dp, kTileN) || !make_map(&mBl, Tl, tf32, n, dp, kTileN))
-    return fail(NAJA_ERR_CUDA, "naja_backmap_noalloc: cuTensorMapEncodeTiled failed");
-  TcArgs a;
-  a.n = n;
-  a.kslices = dp * esz / kSliceBytes;
-  a.N = N;
-  a.tiles_n = (n + kTileN - 1) / kTileN;
-  a.tiles = ((N + kTileM - 1) / kTileM) * a.tiles_n;
-  a.shift = shift;
-  a.V = V;
-  a.v_f64 = v_dtype == NAJA_DTYPE_F64;
-  a.err = err;
-  const size_t smem = kStages * kStageBytes + 1024 + 256 + 4 * 32 * 33 * sizeof(float);
-  int sms = 148, dev = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = static_cast<int>(std::min<long long>(sms, a.tiles));
-  auto kern = tf32 ? backmap_tc_kernel<true> : backmap_tc_kernel<false>;
-  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_backmap_noalloc: ") + cudaGetErrorString(e));
-  kern<<<grid, kThreads, smem, stream>>>(mAh, mAl, mBh, mBl, a);
-  e = cudaGetLastError();
-  if (e != cudaSuccess)
-    return fail(NAJA_ERR_CUDA, std::string("naja_backmap_noalloc: launch failed: ") + cudaGetErrorString(e));
-  int w[4] = {0, 0, 0, 0};
-  e = cudaMemcpyAsync(w, err, sizeof(w), cudaMemcpyDeviceToHost, stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-  if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("naja_backmap_noalloc: ") + cudaGetErrorString(e));
-  if (w[0] != 0)
-    return fail(NAJA_ERR_DEVICE, "naja_backmap_noalloc: tensor-core pipeline gave up a bounded wait (code " +
-                                     std::to_string(w[0]) + ")");
-  return NAJA_OK;
+  if ((st = backmap_tc_split_T(n, d, T, ldt, Th, Tl, mode, stream))) return st;
+  if ((st = backmap_tc_enqueue(n, d, N, Y, y_dtype, Th, Tl, Yh, Yl, shift, V, v_dtype, mode, err, stream))) return st;
+  return backmap_tc_read_error(err, stream, "naja_backmap_noalloc");
 }
 
 }  // namespace naja

@@ -29,14 +29,34 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
-bool is_device_ptr(const void* p) {
-  if (!p) return false;
+int ptr_location(const void* p) {
+  if (!p) return 0;
   cudaPointerAttributes attr;
   if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
     cudaGetLastError();
-    return false;
+    return 0;
   }
-  return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+  if (attr.type == cudaMemoryTypeManaged) return 1;
+  if (attr.type != cudaMemoryTypeDevice) return 0;
+  int cur = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess) {
+    cudaGetLastError();
+    return -1;
+  }
+  return attr.device == cur ? 1 : -1;
+}
+
+bool is_device_ptr(const void* p) { return ptr_location(p) != 0; }
+
+int require_local(const char* fn, std::initializer_list<const void*> ptrs) {
+  int k = 0;
+  for (const void* p : ptrs) {
+    if (ptr_location(p) < 0)
+      return fail(NAJA_ERR_INVALID_ARGUMENT, std::string(fn) + ": pointer argument " + std::to_string(k) +
+                                                 " is device memory of another GPU than the one the call runs on");
+    ++k;
+  }
+  return NAJA_OK;
 }
 
 DeviceGuard::DeviceGuard(int device) {
@@ -153,6 +173,10 @@ struct naja_polytope {
   std::mutex sparse_mu;
   SparseStore sp;
 };
+
+namespace naja {
+int polytope_device(const naja_polytope* P) { return P ? P->device : 0; }
+}  // namespace naja
 
 namespace sparse_build {
 
@@ -416,6 +440,7 @@ int naja_polytope_create(int device, int m, int d, const double* A, int lda, con
   if (lda < m) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_polytope_create: lda < m");
   DeviceGuard g(device);
   if (!g.ok()) return fail(NAJA_ERR_CUDA, "naja_polytope_create: cannot select device");
+  if (int st = require_local("naja_polytope_create", {A, b})) return st;
   naja_polytope* P = new naja_polytope();
   P->device = device;
   P->m = m;
@@ -529,6 +554,9 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
 
   DeviceGuard g(P->device);
   if (!g.ok()) return fail(NAJA_ERR_CUDA, "naja_chr_run: cannot select device");
+  if (int st = require_local("CoordinateHitAndRun", {X0, samples, X_final, p->pair_i, p->pair_j, p->pair_c,
+                                                      p->pair_s, p->rng_state, p->wait_cycles}))
+    return st;
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
 
   ChrLaunchConfig cfg;
@@ -625,8 +653,9 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
 
 int naja_mrg_init_states(int device, unsigned long long seed, int chain_base, int nchains, void* states) {
   if (nchains <= 0 || !states) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_mrg_init_states: bad arguments");
-  if (!is_device_ptr(states)) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_mrg_init_states: states must be device memory");
   DeviceGuard g(device);
+  if (!is_device_ptr(states)) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_mrg_init_states: states must be device memory");
+  if (int st = require_local("naja_mrg_init_states", {states})) return st;
   int st = mrg_init_states(seed, chain_base, nchains, states, 0);
   if (st) return fail(st, "naja_mrg_init_states: launch failed");
   cudaError_t e = cudaDeviceSynchronize();
@@ -637,6 +666,7 @@ int naja_mrg_init_states(int device, unsigned long long seed, int chain_base, in
 int naja_mrg_tape(int device, unsigned long long seed, int chain_base, int nchains, long long count, double* tape) {
   if (nchains <= 0 || count <= 0 || !tape) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_mrg_tape: bad arguments");
   DeviceGuard g(device);
+  if (int st = require_local("naja_mrg_tape", {tape})) return st;
   DeviceBuffer buf;
   void* dt = tape;
   const size_t bytes = static_cast<size_t>(nchains) * count * sizeof(double);
@@ -716,6 +746,12 @@ int prep_batch(int nmodels, const naja_polytope* const* models, const naja_chr_p
     m_max = std::max(m_max, P->m);
   }
   if (ldx < d) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: ldx < d");
+  {
+    DeviceGuard g(models[0]->device);
+    if (int st = require_local("naja_chr_run_batched", {p->pair_i, p->pair_j, p->pair_c, p->pair_s})) return st;
+    for (int k = 0; k < nmodels; ++k)
+      if (int st = require_local("naja_chr_run_batched (X0s[k], samples[k])", {X0s[k], samples[k]})) return st;
+  }
   BatchConfig cfg;
   std::memset(&cfg, 0, sizeof(cfg));
   cfg.threads = c->threads;

@@ -326,6 +326,7 @@ int naja_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, i
     return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_gemm_bf16: BF16 rows must be 16-byte aligned with pitch >= K");
   if ((epi->c_f32 && epi->ldc < N) || (epi->act && epi->ld_act < N) || (epi->act_t && epi->ld_act_t < M))
     return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_gemm_bf16: epilogue pitch too small");
+  if (int st = require_local("naja_gemm_bf16", {A, B, epi->bias, epi->c_f32, epi->act, epi->act_t})) return st;
   CUtensorMap mA, mB;
   if (!tc::make_map_bf16(&mA, A, M, K, lda, kTileM) || !tc::make_map_bf16(&mB, B, N, K, ldb, kTileN))
     return fail(NAJA_ERR_CUDA, "naja_gemm_bf16: cuTensorMapEncodeTiled failed");
@@ -366,6 +367,7 @@ int naja_cast_bf16(int rows, int cols, const float* src, int ld_src, void* dst, 
                    int ld_dst_t, void* stream) {
   if (rows <= 0 || cols <= 0 || !src || ld_src < cols || (dst && ld_dst < cols) || (dst_t && ld_dst_t < rows))
     return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_cast_bf16: bad arguments");
+  if (int st = require_local("naja_cast_bf16", {src, dst, dst_t})) return st;
   const long long total = static_cast<long long>(rows) * cols;
   cast_bf16_kernel<<<grid_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       rows, cols, src, ld_src, static_cast<__nv_bfloat16*>(dst), ld_dst, static_cast<__nv_bfloat16*>(dst_t), ld_dst_t);
@@ -376,6 +378,7 @@ int naja_gelu_backward(int rows, int cols, const float* dact, const float* pre, 
                        int ld_bf, void* dpre_bf_t, int ld_bf_t, void* stream) {
   if (rows <= 0 || cols <= 0 || !dact || !pre || ld < cols || (dpre_bf && ld_bf < cols) || (dpre_bf_t && ld_bf_t < rows))
     return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_gelu_backward: bad arguments");
+  if (int st = require_local("naja_gelu_backward", {dact, pre, dpre, dpre_bf, dpre_bf_t})) return st;
   const long long total = static_cast<long long>(rows) * cols;
   gelu_backward_kernel<<<grid_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       rows, cols, dact, pre, ld, dpre, static_cast<__nv_bfloat16*>(dpre_bf), ld_bf,
@@ -388,6 +391,7 @@ int naja_mse_grad(int rows, int cols, const float* out, const float* target, int
   if (rows <= 0 || cols <= 0 || !out || !target || !loss || ld < cols || (grad_bf && ld_bf < cols) ||
       (grad_bf_t && ld_bf_t < rows))
     return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_mse_grad: bad arguments");
+  if (int st = require_local("naja_mse_grad", {out, target, w, loss, grad, grad_bf, grad_bf_t})) return st;
   const long long total = static_cast<long long>(rows) * cols;
   mse_grad_kernel<<<grid_for(total), 256, 0, static_cast<cudaStream_t>(stream)>>>(
       rows, cols, out, target, ld, w, loss, grad, static_cast<__nv_bfloat16*>(grad_bf), ld_bf,
@@ -397,6 +401,7 @@ int naja_mse_grad(int rows, int cols, const float* out, const float* target, int
 
 int naja_col_sum(int rows, int cols, const float* d, int ld, float* db, void* stream) {
   if (rows <= 0 || cols <= 0 || !d || !db || ld < cols) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_col_sum: bad arguments");
+  if (int st = require_local("naja_col_sum", {d, db})) return st;
   col_sum_kernel<<<(cols + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(rows, cols, d, ld, db);
   return launch_status("naja_col_sum");
 }
@@ -406,6 +411,7 @@ int naja_adam(int rows, int cols, float* W, const float* g, float* m, float* v, 
   if (rows <= 0 || cols <= 0 || !W || !g || !m || !v || ld < cols || step < 1 || (w_bf && ld_bf < cols) ||
       (w_bf_t && ld_bf_t < rows))
     return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_adam: bad arguments");
+  if (int st = require_local("naja_adam", {W, g, m, v, w_bf, w_bf_t})) return st;
   const float c1 = 1.0f / (1.0f - std::pow(beta1, static_cast<float>(step)));
   const float c2 = 1.0f / (1.0f - std::pow(beta2, static_cast<float>(step)));
   const long long total = static_cast<long long>(rows) * cols;

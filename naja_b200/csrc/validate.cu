@@ -190,6 +190,7 @@ extern "C" int naja_validate(const float* samples, long long N, int dim, int nch
   if (spc > kEssMaxSeries)
     return fail(NAJA_ERR_UNSUPPORTED, "naja_validate: more than " + std::to_string(kEssMaxSeries) +
                                           " samples per chain");
+  if (int st = require_local("naja_validate", {samples, ess, rhat})) return st;
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
   DeviceBuffer bs, be, br;
   const void* ds = nullptr;

@@ -1,11 +1,13 @@
 """Sampling with the backmap and the copy to host overlapped.
 
-`sample_backmapped` is the job of `naja sample run --backmap` as one call:
-CHR samples of a polytope, mapped to reaction space (v = T y + shift) and
-delivered into a host buffer.  The chains run in chunks; while the step
-kernel of chunk k + 1 runs on one stream (one CTA per chain, a few SMs), the
-backmap of chunk k runs on the tensor cores of the other SMs and its rows
-are copied to the host on a second stream.
+`sample_backmapped` is the job of `naja sample run --backmap` as one call
+(naja_chr_run_backmapped in the C ABI): CHR samples of a polytope, mapped to
+reaction space (v = T y + shift) and delivered into a host buffer.  The
+chains run in chunks; while the step kernel of chunk k + 1 runs on one
+stream (one CTA per chain, a few SMs), the backmap of chunk k runs on the
+tensor cores of the other SMs and its rows are copied to the host on a
+second stream.  The library queues chunk k + 1 before chunk k's backmap, so
+the step kernel never waits for the host.
 
 A chunk boundary falls on a multiple of both the resync interval and the
 thinning.  There a single run recomputes the slack from x in FP64 anyway,
@@ -17,11 +19,14 @@ interval, or with the MRG32k3a streams, the job runs as one chunk.
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 
 import numpy as np
 
-from .sampler import Polytope, backmap
+from . import _lib
+from ._lib import check, load
+from .sampler import _BACKMAP, Polytope, _is_torch, _ptr
 
 try:
     import torch
@@ -31,8 +36,9 @@ except Exception:  # pragma: no cover
 
 def chunk_samples(nspc: int, thinning: int, resync_interval: int, rng: str = "philox",
                   target_steps: int = 1 << 16) -> int:
-    """Samples per chunk: whole periods of lcm(resync, thinning) steps, about
-    `target_steps` steps long; all of nspc when the job cannot be split."""
+    """Samples per chunk the library picks: whole periods of lcm(resync,
+    thinning) steps, about `target_steps` steps long; all of nspc when the
+    job cannot be split."""
     if resync_interval <= 0 or rng != "philox":
         return int(nspc)
     period = math.lcm(int(resync_interval), int(thinning)) // int(thinning)
@@ -42,63 +48,49 @@ def chunk_samples(nspc: int, thinning: int, resync_interval: int, rng: str = "ph
 
 def sample_backmapped(P: Polytope, T, shift, X0, nspc: int, thinning: int, nchains: int, out, *,
                       mode: str = "tf32x3", chunk: int | None = None, resync_interval: int = 0,
-                      rng: str = "philox", **kw):
+                      rng: str = "philox", samples=None, stream=None, **kw):
     """Runs `nchains` chains of `nspc` samples from X0 ((nchains, d) or (d,))
     and writes v = T y + shift for every sample into `out`, a (nspc * nchains,
-    n) float32 host tensor (pinned for the copies to overlap), rows in the
-    sample order of naja_chr_run.  Returns the final positions (nchains, d)
-    on the device.  Extra keywords go to Polytope.run (seed, pair_prob,
-    precision, sparse, ...)."""
-    if torch is None:
-        raise RuntimeError("sample_backmapped needs torch")
-    if "step_offset" in kw or "out_nchains" in kw or "chain_base" in kw:
-        raise ValueError("sample_backmapped runs whole jobs: no step_offset, chain_base or out_nchains")
-    dev = torch.device("cuda", P.device)
+    n) float32 or float64 array or tensor (pinned host memory for the copies
+    to overlap), rows in the sample order of naja_chr_run.  `samples`
+    (optional, (nspc * nchains, d)) also receives the samples.  Returns the
+    final positions (nchains, d) as float64 (a CUDA tensor when torch is
+    present).  Extra keywords go to Polytope.params (seed, pair_prob,
+    precision, sparse, out_dtype, ...)."""
+    if "out_nchains" in kw or "chain_base" in kw:
+        raise ValueError("sample_backmapped runs whole jobs: no chain_base or out_nchains")
     d = P.d
-
-    def on_device(v):
-        t = v if torch.is_tensor(v) else torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64))
-        return t.to(device=dev, dtype=torch.float64)
-
-    T_dev, sh_dev = on_device(T), on_device(shift)
-    n = T_dev.shape[0]
+    Tn = T if (_is_torch(T) and T.is_cuda) else np.asfortranarray(np.asarray(T, dtype=np.float64))
+    n, dT = int(T.shape[0]), int(T.shape[1])
+    if dT != d:
+        raise _lib.InvalidArgument(1, "backmap_into: transformation shape mismatch with samples")
+    # column-major T: a Fortran-ordered array, or for a CUDA tensor the row-major T^T
+    Tc = Tn.to(torch.float64).t().contiguous() if _is_torch(Tn) else Tn
+    sh = shift.to(torch.float64).contiguous() if _is_torch(shift) else np.ascontiguousarray(
+        np.asarray(shift, dtype=np.float64).reshape(-1))
     if tuple(out.shape) != (nspc * nchains, n):
         raise ValueError(f"out must be ({nspc * nchains}, {n})")
-    X = torch.as_tensor(X0, dtype=torch.float64).to(dev)
-    if X.dim() == 1:
-        X = X.expand(nchains, d)
-    X = X.contiguous().clone()
-    cs = int(chunk) if chunk else chunk_samples(nspc, thinning, resync_interval, rng)
-    if cs < nspc and (resync_interval <= 0 or (cs * thinning) % resync_interval or rng != "philox"):
-        raise ValueError("a chunk must span whole resync intervals of a Philox run")
-    rows = cs * nchains
-    samples = [torch.empty((rows, d), dtype=torch.float32, device=dev) for _ in range(2)]
-    V = [torch.empty((rows, n), dtype=torch.float32, device=dev) for _ in range(2)]
-    xs = [X, torch.empty_like(X)]
-    s_chr = torch.cuda.Stream(dev)
-    s_bm = torch.cuda.Stream(dev)
-    s_chr.wait_stream(torch.cuda.current_stream(dev))
-    s_bm.wait_stream(torch.cuda.current_stream(dev))
-    freed = [None, None]  # event: chunk k - 2's backmap and copy are done with buffer k % 2
-    for k, s0 in enumerate(range(0, nspc, cs)):
-        ns = min(cs, nspc - s0)
-        b = k % 2
-        r = ns * nchains
-        with torch.cuda.stream(s_chr):
-            if freed[b] is not None:
-                s_chr.wait_event(freed[b])
-            P.run(xs[k % 2], ns, thinning, nchains, out=samples[b][:r], X_final=xs[(k + 1) % 2],
-                  step_offset=s0 * thinning, resync_interval=resync_interval, rng=rng, **kw)
-            done = torch.cuda.Event()
-            done.record(s_chr)
-        with torch.cuda.stream(s_bm):
-            s_bm.wait_event(done)
-            backmap(T_dev, sh_dev, samples[b][:r], mode=mode, out=V[b][:r])
-            out[s0 * nchains:s0 * nchains + r].copy_(V[b][:r], non_blocking=True)
-            freed[b] = torch.cuda.Event()
-            freed[b].record(s_bm)
-    torch.cuda.current_stream(dev).wait_stream(s_bm)
-    torch.cuda.current_stream(dev).wait_stream(s_chr)
-    torch.cuda.synchronize(dev)
-    P.check()
-    return xs[len(range(0, nspc, cs)) % 2]
+    vdt = _lib.DTYPE_F64 if str(out.dtype) in ("float64", "torch.float64") else _lib.DTYPE_F32
+    if _is_torch(X0):
+        X = X0.to(torch.float64)
+        if X.dim() == 1:
+            X = X.expand(nchains, d)
+        X = X.contiguous()
+    else:
+        X = np.asarray(X0, dtype=np.float64)
+        if X.ndim == 1:
+            X = np.broadcast_to(X, (nchains, d))
+        X = np.ascontiguousarray(X)
+    if torch is not None:
+        dev = torch.device("cuda", P.device)
+        Xf = torch.empty((nchains, d), dtype=torch.float64, device=dev)
+        if stream is None:
+            stream = torch.cuda.current_stream(dev).cuda_stream
+    else:
+        Xf = np.empty((nchains, d), dtype=np.float64)
+    p, keep = P.params(nspc, thinning, nchains, resync_interval=resync_interval, rng=rng, **kw)
+    check(load().naja_chr_run_backmapped(P._h, C.byref(p), _ptr(X), d, n, _ptr(Tc), n, _ptr(sh), _BACKMAP[mode],
+                                         _ptr(out), vdt, _ptr(samples), _ptr(Xf), int(chunk or 0),
+                                         None if stream is None else C.c_void_p(int(stream))))
+    del keep
+    return Xf

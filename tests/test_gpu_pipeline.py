@@ -34,3 +34,43 @@ def test_chunked_job_equals_one_launch(cuda, sparse):
     torch.cuda.synchronize()
     assert torch.equal(out, ref.cpu())
     assert np.array_equal(xf.cpu().numpy(), xf1)
+
+
+@pytest.mark.parametrize("mode", ["fp64", "bf16x3"])
+def test_device_outputs_and_samples(cuda, mode):
+    """V and the samples in device memory (no copies), pageable numpy T / shift,
+    another backmap mode: the same rows as one launch followed by the backmap."""
+    import torch
+
+    g = synth.genome_shaped(n=300, d=90, density=0.1, seed_T=9, seed_u=10)
+    P = Polytope(g["A"], g["b"])
+    nspc, thin, nch, K = 60, 6, 5, 36  # chunks of 18 samples = 3 resync periods, last chunk partial
+    kw = dict(seed=4, pair_prob=0.3, precision="fp32")
+    n, d = g["T"].shape
+    out = torch.empty((nspc * nch, n), dtype=torch.float32, device=cuda)
+    S = torch.empty((nspc * nch, d), dtype=torch.float32, device=cuda)
+    sample_backmapped(P, g["T"], g["shift"], g["start"], nspc, thin, nch, out, mode=mode, chunk=18,
+                      resync_interval=K, samples=S, **kw)
+    Y = P.run(g["start"], nspc, thin, nch, resync_interval=K, **kw)
+    assert np.array_equal(S.cpu().numpy(), Y)
+    ref = backmap(g["T"], g["shift"], Y, mode=mode)
+    assert np.array_equal(out.cpu().numpy(), ref)
+
+
+def test_pageable_host_output_and_rejections(cuda):
+    g = synth.genome_shaped(n=200, d=60, density=0.1, seed_T=11, seed_u=12)
+    P = Polytope(g["A"], g["b"])
+    nspc, thin, nch = 40, 5, 3
+    out = np.empty((nspc * nch, g["T"].shape[0]), dtype=np.float64)
+    sample_backmapped(P, g["T"], g["shift"], g["start"], nspc, thin, nch, out, mode="fp64", chunk=10,
+                      resync_interval=25, seed=1)
+    Y = P.run(g["start"], nspc, thin, nch, resync_interval=25, seed=1)
+    assert np.array_equal(out, backmap(g["T"], g["shift"], Y, mode="fp64", out_dtype=np.float64))
+    from naja_b200._lib import InvalidArgument
+
+    with pytest.raises(InvalidArgument):  # a chunk of 7 samples is not a whole number of resync periods
+        sample_backmapped(P, g["T"], g["shift"], g["start"], nspc, thin, nch, out, mode="fp64", chunk=7,
+                          resync_interval=25, seed=1)
+    with pytest.raises(InvalidArgument):  # MRG streams cannot be chunked
+        sample_backmapped(P, g["T"], g["shift"], g["start"], nspc, thin, nch, out, mode="fp64", chunk=10,
+                          resync_interval=25, rng="mrg")

@@ -8,8 +8,10 @@ library.  The test calls it through the C ABI twice in a row with different
 inputs (the array is reused, so the second call must not see the first
 call's data) and compares each result with the allocating entry point,
 naja_backmap, in the same mode, within the backmap tests' tolerance
-(2^-15 of |T||y| + |shift| for BF16X3, 2^-17 for TF32X3).  It runs alone in
-a fresh process as well as after the other tests.
+(2^-15 of |T||y| + |shift| for BF16X3, 2^-17 for TF32X3), and checks around
+warm calls that no device memory is taken: free device memory, torch's
+allocator and the default stream-ordered pool stay as they were.  It runs
+alone in a fresh process as well as after the other tests.
 """
 import ctypes as C
 
@@ -85,3 +87,59 @@ def test_noalloc_rejects_oversized_and_host_buffers(cuda):
                                   C.c_void_p(Yd.data_ptr()), _lib.DTYPE_F32, C.c_void_p(host_out.ctypes.data),
                                   _lib.DTYPE_F32, MODE["tf32x3"], stream)
     assert st == _lib.NAJA_ERR_INVALID_ARGUMENT
+
+
+def _pool_usage(dev_index):
+    """(used, reserved) bytes of the device's default memory pool (the pool
+    cudaMallocAsync draws from), read through the driver API."""
+    cu = C.CDLL("libcuda.so.1")
+    dev = C.c_int()
+    assert cu.cuDeviceGet(C.byref(dev), dev_index) == 0
+    pool = C.c_void_p()
+    assert cu.cuDeviceGetDefaultMemPool(C.byref(pool), dev) == 0
+    used, reserved = C.c_uint64(), C.c_uint64()
+    assert cu.cuMemPoolGetAttribute(pool, 7, C.byref(used)) == 0  # CU_MEMPOOL_ATTR_USED_MEM_CURRENT
+    assert cu.cuMemPoolGetAttribute(pool, 5, C.byref(reserved)) == 0  # CU_MEMPOOL_ATTR_RESERVED_MEM_CURRENT
+    return used.value, reserved.value
+
+
+def test_noalloc_allocates_no_device_memory(cuda):
+    """Around a warm call: the device's free memory, torch's allocator and the
+    default stream-ordered pool are unchanged, while the allocating entry
+    point in the same place draws from that pool."""
+    import torch
+
+    from naja_b200 import _lib
+
+    lib = _lib.load()
+    N, n, d = 2000, 500, 100
+    T, Y, shift, Tc, Yd, sd = _inputs(5, N, n, d)
+    out = torch.empty((N, n), dtype=torch.float32, device=cuda)
+    stream = C.c_void_p(torch.cuda.current_stream(cuda).cuda_stream)
+    args = (n, d, N, C.c_void_p(Tc.data_ptr()), n, C.c_void_p(sd.data_ptr()), C.c_void_p(Yd.data_ptr()),
+            _lib.DTYPE_F32, C.c_void_p(out.data_ptr()), _lib.DTYPE_F32, MODE["bf16x3"], stream)
+    _lib.check(lib.naja_backmap_noalloc(*args))  # warm: set-up done, kernels loaded
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(cuda)[0]
+    torch0 = (torch.cuda.memory_allocated(cuda), torch.cuda.memory_reserved(cuda))
+    pool0 = _pool_usage(cuda.index or 0)
+    for _ in range(3):
+        _lib.check(lib.naja_backmap_noalloc(*args))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(cuda)[0] == free0
+    assert (torch.cuda.memory_allocated(cuda), torch.cuda.memory_reserved(cuda)) == torch0
+    assert _pool_usage(cuda.index or 0) == pool0
+    # the allocating entry point does draw its split operands from the pool
+    # (its high-water mark must exceed them; current usage returns after the call)
+    cu = C.CDLL("libcuda.so.1")
+    dev = C.c_int()
+    cu.cuDeviceGet(C.byref(dev), cuda.index or 0)
+    pool = C.c_void_p()
+    cu.cuDeviceGetDefaultMemPool(C.byref(pool), dev)
+    zero = C.c_uint64(0)
+    assert cu.cuMemPoolSetAttribute(pool, 8, C.byref(zero)) == 0  # reset CU_MEMPOOL_ATTR_USED_MEM_HIGH
+    _lib.check(lib.naja_backmap(*args))
+    torch.cuda.synchronize()
+    high = C.c_uint64()
+    assert cu.cuMemPoolGetAttribute(pool, 8, C.byref(high)) == 0
+    assert high.value >= 2 * N * 128 * 2  # two BF16 halves of the samples, d padded to 128
