@@ -351,6 +351,8 @@ def _ours(a, rank, world):
         line["cpu_baseline"] = _cpu_baseline(W, a, min_ess / W.steps)
     if rank == 0 and a.batch_models > 0:
         line["batched"] = _batched(a, torch, dev)
+    if rank == 0 and a.gate_budget_s > 0:
+        line["gate_run"] = _gate(a)
     if rank == 0 and a.learned_train > 0:
         line["learned_rounding"], detail["learned_rounding"] = _learned(a)
     if rank == 0 and a.detail_file:
@@ -444,6 +446,35 @@ def _batched(a, torch, dev):
                          "peak_source": src, "bytes_per_chr_step": bytes_total / steps},
             "autotune_top": sorted(({"shape": str(k), "M_steps_per_s": v / 1e6} for k, v in table.items()),
                                    key=lambda r: -r["M_steps_per_s"])[:5]}
+
+
+def _gate(a):
+    """The metric at its gate: the genome-shaped workload's 16 chains
+    (thinning 116, pair-prob 0.3, resync 2048, FP32 tier, Philox seed 0)
+    continued chunk by chunk (12,500 samples per chain per chunk) until
+    split-R-hat < 1.01 with no bound violations, or until the time budget;
+    per rounding: plain (none), the reference's Dikin preconditioner, the
+    whole-ellipsoid Dikin rounding, and the latter refined once to the
+    samples' isotropic position after two warm-up chunks.  Seconds include
+    computing the rounding, every chunk's sampling and back-map to y, and the
+    R-hat checks; min-ESS is over the samples that count (after the warm-up)."""
+    from naja_b200 import gate, synth
+
+    g = synth.genome_shaped(n=a.n, d=a.d, density=0.08, seed_T=0, seed_u=1)
+    out = {"workload": f"genome-shaped n={a.n} d={a.d}, {a.nchains} chains, chunks of {a.nspc} samples x thinning "
+                       f"{a.thinning}, pair-prob {a.pair_prob}, until split-R-hat < 1.01 or {a.gate_budget_s:.0f} s",
+           "methods": {}}
+    for method, adapt in (("none", 0), ("dikin", 0), ("dikin_full", 0), ("dikin_full", 2)):
+        r = gate.sample_to_gate(g["A"], g["b"], g["start"], method=method, adapt_after=adapt, nchains=a.nchains,
+                                thinning=a.thinning, chunk_nspc=a.nspc, pair_prob=a.pair_prob,
+                                resync_interval=a.resync, seed=a.seed, budget_s=a.gate_budget_s)
+        r["curve"] = [[round(c["seconds"], 2), round(c["rhat_max"], 4)] for c in r["curve"]]
+        out["methods"][r["method"]] = r
+    m = out["methods"]
+    best = max(m.values(), key=lambda r: (r["reached"], r["min_ess_per_s"]))
+    out["best"] = best["method"]
+    out["reached"] = [k for k, r in m.items() if r["reached"]]
+    return out
 
 
 def _precision_study(a):
@@ -724,6 +755,8 @@ def main(argv=None):
     ap.add_argument("--no-fp64-figure", dest="fp64_figure", action="store_false",
                     help="skip the FP64-tier figure of the same job")
     ap.add_argument("--no-cube", dest="cube", action="store_false", help="skip the unit-cube workload")
+    ap.add_argument("--gate-budget-s", type=float, default=60.0,
+                    help="run-to-gate section: seconds per rounding method (0 = skip)")
     ap.add_argument("--detail-file", default="",
                     help="write per-step times and per-variant records here (JSON)")
     ap.add_argument("--precision-study", action="store_true",

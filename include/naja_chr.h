@@ -233,7 +233,9 @@ int naja_chr_run_backmapped(const naja_polytope* P, const naja_chr_params* param
  * row-major float32 sample matrix (src/validate/mcmc.cpp:91-194).
  * layout 0 = the reference's windows (chain c = rows [c*spc, (c+1)*spc)),
  * layout 1 = chains interleaved as the sampler writes them (row r belongs
- * to chain r % nchains).  ess: dim*nchains values (dim-major), rhat: dim. */
+ * to chain r % nchains).  ess: dim*nchains values (dim-major), rhat: dim;
+ * either may be null (that metric is skipped).  ESS takes at most 49,152
+ * samples per chain (a series is held on chip); R-hat has no such limit. */
 int naja_validate(const float* samples, long long N, int dim, int nchains, int layout, double* ess,
                   double* rhat, void* stream);
 

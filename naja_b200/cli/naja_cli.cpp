@@ -12,19 +12,30 @@
 //       (src/engine/profile.h:28-66), config_used.txt (job_sampling.cu:34-60).
 //       Thinning defaults to max(d/6, 1) and the seed to the reference's hash
 //       of model name, model directory and GPU (job_sampling.cu:237-254).
+//       Rounding inputs (src/rounding/plan.cpp:12-62): --pair-schedule FILE
+//       (i,j,c,s CSV) or --iter-rounding-passes P --iter-rounding-warmup W (a
+//       warm-up estimate, src/rounding/runtime_warmup.cpp:16-108) select
+//       Jacobi-rotated pair steps; --affine-hull-tol samples the affine hull of
+//       the rows tight at the start (job_sampling.cu:196-235, T and shift
+//       composed as in :299-303); --extra-constraint-eps / --constraint-eps
+//       relax rows as job_sampling.cu:138-146 does.
+//   naja sample calibrate-rounding --models-root DIR --model-list FILE --out F.csv
+//       src/cli/sample/cmd_calibrate_rounding.cpp:24-195: one pair schedule
+//       from warm-up moments pooled over a list of models.
 //   naja validate --samples F.npy [--model-dir DIR] [--n-chains 4]
 //       src/cli/validate_cli.cpp:49-296: ESS / split-R-hat (naja_validate, the
 //       reference's chain windows), bounds compliance of v = T y + shift
 //       against the GEM bounds (src/validate/bounds_check.cpp:8-39), the
 //       one-line status to stderr and the JSON report to stdout.
 //
-// Flags the reference accepts for features this project leaves out
-// (iterative rounding passes, affine-hull reduction, the cube-centre start
-// LP) are rejected with a usage error instead of being ignored.
+// The one flag value the reference accepts for a feature this project leaves
+// out (--start-policy cube_center, a Gurobi LP) is rejected with a usage
+// error instead of being ignored.
 #include <sys/stat.h>
 #include <unistd.h>
 
 #include <algorithm>
+#include <charconv>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -39,8 +50,10 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
+#include "../../include/naja/rounding.hpp"
 #include "../../include/naja_chr.h"
 
 namespace {
@@ -82,43 +95,85 @@ std::string self_path() {
   return buf;
 }
 
-// CSV of numbers; rows separated by newlines, values by commas.
+// CSV of numbers; rows separated by newlines, values by commas.  The text is
+// split into line-aligned blocks parsed in parallel (std::from_chars), one
+// thread per block -- the reference parses cell by cell with std::stod on one
+// thread (src/csv_loader.h:12-49), which dominates loading at genome scale.
 struct Csv {
   int rows = 0, cols = 0;
   std::vector<double> v;  // row-major
 };
+namespace csv_detail {
+struct Block {
+  std::vector<double> v;
+  std::vector<int> row_cols;
+  std::string error;
+};
+inline bool blank(char ch) { return ch == ' ' || ch == '\t' || ch == '\r'; }
+void parse_block(const char* p, const char* end, Block& out) {
+  while (p < end) {
+    const char* eol = static_cast<const char*>(std::memchr(p, '\n', end - p));
+    if (!eol) eol = end;
+    const char* q = p;
+    while (q < eol && (blank(*q) || *q == '\f' || *q == '\v')) ++q;
+    if (q < eol) {
+      int cols = 0;
+      while (q < eol) {
+        if (*q == '+') ++q;
+        double x = 0.0;
+        const auto r = std::from_chars(q, eol, x);
+        if (r.ec != std::errc() || r.ptr == q) {
+          out.error = "bad number";
+          return;
+        }
+        out.v.push_back(x);
+        ++cols;
+        q = r.ptr;
+        while (q < eol && blank(*q)) ++q;
+        if (q < eol && *q == ',') ++q;
+        while (q < eol && blank(*q)) ++q;
+      }
+      out.row_cols.push_back(cols);
+    }
+    p = eol + 1;
+  }
+}
+}  // namespace csv_detail
 Csv load_csv(const std::string& path) {
   std::ifstream f(path, std::ios::binary);
   if (!f.is_open()) throw std::runtime_error("cannot open file: " + path);
   std::string text((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+  const char* beg = text.data();
+  const char* end = beg + text.size();
+  const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nblk = std::max<size_t>(1, std::min<size_t>(hw, text.size() / (1 << 20)));
+  std::vector<const char*> cut(nblk + 1, end);
+  cut[0] = beg;
+  for (size_t k = 1; k < nblk; ++k) {
+    const char* at = beg + text.size() * k / nblk;
+    const char* nl = static_cast<const char*>(std::memchr(at, '\n', end - at));
+    cut[k] = nl ? nl + 1 : end;
+    if (cut[k] < cut[k - 1]) cut[k] = cut[k - 1];
+  }
+  std::vector<csv_detail::Block> blocks(nblk);
+  std::vector<std::thread> pool;
+  for (size_t k = 1; k < nblk; ++k)
+    pool.emplace_back([&, k] { csv_detail::parse_block(cut[k], cut[k + 1], blocks[k]); });
+  csv_detail::parse_block(cut[0], cut[1], blocks[0]);
+  for (auto& t : pool) t.join();
   Csv c;
-  const char* p = text.c_str();
-  const char* end = p + text.size();
-  while (p < end) {
-    const char* eol = static_cast<const char*>(std::memchr(p, '\n', end - p));
-    if (!eol) eol = end;
-    int cols = 0;
-    const char* q = p;
-    bool any = false;
-    for (const char* s = p; s < eol; ++s)
-      if (!std::isspace(static_cast<unsigned char>(*s))) any = true;
-    if (any) {
-      while (q < eol) {
-        char* next = nullptr;
-        const double x = std::strtod(q, &next);
-        if (next == q) throw std::runtime_error("bad number in " + path + " at row " + std::to_string(c.rows + 1));
-        c.v.push_back(x);
-        ++cols;
-        q = next;
-        while (q < eol && (*q == ' ' || *q == '\t' || *q == '\r')) ++q;
-        if (q < eol && *q == ',') ++q;
-        while (q < eol && (*q == ' ' || *q == '\t' || *q == '\r')) ++q;
-      }
+  size_t total = 0;
+  for (const auto& b : blocks) total += b.v.size();
+  c.v.reserve(total);
+  for (const auto& b : blocks) {
+    if (!b.error.empty())
+      throw std::runtime_error(b.error + " in " + path + " near row " + std::to_string(c.rows + b.row_cols.size() + 1));
+    for (int cols : b.row_cols) {
       if (c.rows == 0) c.cols = cols;
       else if (cols != c.cols) throw std::runtime_error("ragged csv: " + path);
       ++c.rows;
     }
-    p = eol + 1;
+    c.v.insert(c.v.end(), b.v.begin(), b.v.end());
   }
   if (c.rows == 0) throw std::runtime_error("empty csv: " + path);
   return c;
@@ -285,7 +340,12 @@ double seconds_since(std::chrono::steady_clock::time_point t0) {
             << "      [--ksparse-prob p] [--ksparse-k k] [--extra-constraints auto|ignore|require]\n"
             << "      [--backmap] [--write-npy] [--bounds-policy ignore|filter] [--bounds-eps e]\n"
             << "      [--write-samples-valid] [--precision fp32|fp64] [--rng philox|mrg]\n"
-            << "      [--backmap-mode fp64|tf32x3|bf16x3] [--verbose] [--quiet] [--dry-run] [--print-config]\n";
+            << "      [--backmap-mode fp64|tf32x3|bf16x3] [--verbose] [--quiet] [--dry-run] [--print-config]\n"
+            << "      [--pair-schedule FILE] [--iter-rounding-passes P] [--iter-rounding-warmup W]\n"
+            << "      [--affine-hull-tol t] [--extra-constraint-eps e] [--constraint-eps e]\n"
+            << "  naja sample calibrate-rounding --models-root <dir> --model-list <file> --out <csv>\n"
+            << "      [--warmup 2000] [--passes 2] [--pair-prob 0.3] [--extra-constraint-eps 0] [--seed 1]\n"
+            << "      [--max-models 0]\n";
   std::exit(2);
 }
 
@@ -298,6 +358,9 @@ struct RunConfig {
   std::string model_dir, model_name, rounding_dir, gem_dir, data_dir, out_dir;
   int gpu = 0, n_chains = -1, n_samples = -1, tpb = 128, thinning = 0, resync_interval = 0, ksparse_k = 8;
   double pair_prob = 0.0, ksparse_prob = 0.0, bounds_eps = 1e-6;
+  int iter_rounding_passes = 0, iter_rounding_warmup = 0;
+  double affine_hull_tol = 0.0, extra_constraint_eps = 0.0, constraint_eps = 0.0;
+  std::string pair_schedule;
   std::string extra_constraints = "auto", bounds_policy = "ignore", precision = "fp32", rng = "philox",
               backmap_mode = "fp64";
   bool backmap = false, write_npy = false, verbose = false, quiet = false, dry_run = false, print_config = false,
@@ -369,7 +432,13 @@ void write_generated_config(const std::string& path, const RunConfig& c) {
     << "WRITE_SAMPLES_VALID=" << (c.write_samples_valid ? 1 : 0) << "\n"
     << "PRECISION=" << c.precision << "\n"
     << "RNG=" << c.rng << "\n"
-    << "BACKMAP_MODE=" << c.backmap_mode << "\n";
+    << "BACKMAP_MODE=" << c.backmap_mode << "\n"
+    << "ITER_ROUNDING_PASSES=" << c.iter_rounding_passes << "\n"
+    << "ITER_ROUNDING_WARMUP=" << c.iter_rounding_warmup << "\n"
+    << "PAIR_SCHEDULE=" << c.pair_schedule << "\n"
+    << "AFFINE_HULL_TOL=" << c.affine_hull_tol << "\n"
+    << "EXTRA_CONSTRAINT_EPS=" << c.extra_constraint_eps << "\n"
+    << "CONSTRAINT_EPS=" << c.constraint_eps << "\n";
 }
 
 void write_run_manifest(const RunConfig& c, const std::vector<std::string>& argv_full) {
@@ -462,12 +531,16 @@ int run_sampling(const RunConfig& c) {
     Csv eA = load_csv(c.file("extra_A")), eb = load_csv(c.file("extra_b"));
     if (eA.cols != A.cols) throw std::runtime_error("extra_A has " + std::to_string(eA.cols) + " columns, A has " + std::to_string(A.cols));
     if (eb.rows * eb.cols != eA.rows) throw std::runtime_error("extra_b length does not match extra_A rows");
+    for (double& v : eb.v) v += c.extra_constraint_eps;  // extra_constraints.cpp: b_extra + eps
     A.v.insert(A.v.end(), eA.v.begin(), eA.v.end());
     A.rows += eA.rows;
     b.v.insert(b.v.end(), eb.v.begin(), eb.v.end());
     b.rows += eb.rows * eb.cols;
   }
-  const int m = A.rows, d = A.cols;
+  if (c.constraint_eps > 0.0)
+    for (double& v : b.v) v += c.constraint_eps;  // global relaxation A x <= b + eps (job_sampling.cu:142-146)
+  int m = A.rows, d = A.cols;
+  const int d_file = d;
   if (static_cast<int>(b.v.size()) != m) throw std::runtime_error("dimension mismatch: rhs vector size (" + std::to_string(b.v.size()) + ") != rows (" + std::to_string(m) + ")");
   if (static_cast<int>(x0.v.size()) != d) throw std::runtime_error("start point has " + std::to_string(x0.v.size()) + " values, A has " + std::to_string(d) + " columns");
   // feasible start (src/validate/feasibility.h:12-35): max(A x0 - b) <= 1e-9
@@ -478,6 +551,46 @@ int run_sampling(const RunConfig& c) {
     worst = std::max(worst, s - b.v[r]);
   }
   if (worst > 1e-9) throw std::runtime_error("infeasible start point: max(A x0 - b) = " + std::to_string(worst));
+  // Affine hull of the rows tight at the start (job_sampling.cu:196-235):
+  // sample z in {z : (A B) z <= b - A x0}, y = B z + x0.
+  std::vector<double> hull_basis, hull_shift;
+  if (c.affine_hull_tol > 0.0) {
+    int dd = d, n_tight = 0;
+    if (naja::rounding::affine_hull_basis(A.v, b.v, x0.v, m, d, c.affine_hull_tol, hull_basis, &dd, &n_tight)) {
+      Csv Ar;
+      Ar.rows = m;
+      Ar.cols = dd;
+      Ar.v.assign(static_cast<size_t>(m) * dd, 0.0);
+      std::vector<double> slack0(m);
+      for (int r = 0; r < m; ++r) {
+        double sx = 0.0;
+        const double* ar = &A.v[static_cast<size_t>(r) * d];
+        for (int k = 0; k < d; ++k) sx += ar[k] * x0.v[k];
+        slack0[r] = b.v[r] - sx;
+        double* o = &Ar.v[static_cast<size_t>(r) * dd];
+        for (int k = 0; k < d; ++k) {
+          const double a = ar[k];
+          if (a == 0.0) continue;
+          const double* brow = &hull_basis[static_cast<size_t>(k) * dd];
+          for (int q = 0; q < dd; ++q) o[q] += a * brow[q];
+        }
+      }
+      hull_shift = x0.v;
+      A = std::move(Ar);
+      b.v = std::move(slack0);
+      x0.v.assign(dd, 0.0);
+      d = dd;
+      if (c.verbose) {
+        std::cout << "  affine_hull_tol  " << std::setprecision(12) << c.affine_hull_tol << "\n"
+                  << "  affine_hull_rows " << n_tight << "\n  affine_hull_dim  " << dd << " (from " << d_file << ")\n";
+      }
+      for (int r = 0; r < m; ++r)
+        if (-b.v[r] > 1e-9) throw std::runtime_error("infeasible start point after the affine-hull reduction");
+    } else if (c.verbose) {
+      std::cout << "  affine_hull_tol  " << std::setprecision(12) << c.affine_hull_tol << " (no reduction; "
+                << n_tight << " tight rows)\n";
+    }
+  }
   const int thinning = c.thinning > 0 ? c.thinning : std::max(d / 6, 1);
   prof.load = seconds_since(t0);
   prof.n_chains = c.n_chains;
@@ -517,6 +630,27 @@ int run_sampling(const RunConfig& c) {
   p.precision = c.precision == "fp64" ? NAJA_PREC_FP64 : NAJA_PREC_FP32;
   p.rng = c.rng == "mrg" ? NAJA_RNG_REF_MRG : NAJA_RNG_PHILOX;
   p.out_dtype = NAJA_DTYPE_F32;
+  // Rounding plan (src/rounding/plan.cpp:12-62): a schedule file, else a warm-up estimate.
+  naja::rounding::PairSchedule sched;
+  if (!c.pair_schedule.empty()) {
+    phase(st, "loading pair schedule");
+    sched = naja::rounding::load_pair_schedule_csv(c.pair_schedule);
+  } else if (c.iter_rounding_passes > 0 && c.iter_rounding_warmup > 0 && d >= 2) {
+    phase(st, "iterative rounding-lite (warmup)");
+    sched = naja::rounding::estimate_runtime_pair_schedule(P, x0.v, seed, c.iter_rounding_passes,
+                                                           c.iter_rounding_warmup, c.pair_prob, p);
+    if (c.verbose)
+      std::cout << "  iter_rounding_passes " << c.iter_rounding_passes << "\n  iter_rounding_warmup "
+                << c.iter_rounding_warmup << "\n  iter_rounding_pairs  " << sched.size() << "\n";
+  }
+  if (sched.size() > 0) {
+    p.pair_mode = 2;
+    p.pair_i = sched.i.data();
+    p.pair_j = sched.j.data();
+    p.pair_c = sched.c.data();
+    p.pair_s = sched.s.data();
+    p.n_pairs = sched.size();
+  }
   const long long N = static_cast<long long>(c.n_samples) * c.n_chains;
   std::vector<float> out;
   long long dim = d;
@@ -524,9 +658,29 @@ int run_sampling(const RunConfig& c) {
   if (c.backmap) {
     phase(st, "loading transform");
     Csv T = load_csv(c.file("T")), sh = load_csv(c.file("shift"));
-    if (T.cols != d) throw std::runtime_error("backmap_into: transformation shape mismatch with samples");
-    Tcm = colmajor(T);
+    if (T.cols != d_file)
+      throw std::runtime_error("dimension mismatch: transform matrix cols (" + std::to_string(T.cols) +
+                               ") != reduced dim (" + std::to_string(d_file) + ")");
     shift = sh.v;
+    if (!hull_basis.empty()) {
+      // T <- T0 B, shift <- T0 x0 + shift (job_sampling.cu:299-303)
+      Csv Tr;
+      Tr.rows = T.rows;
+      Tr.cols = d;
+      Tr.v.assign(static_cast<size_t>(T.rows) * d, 0.0);
+      for (int i = 0; i < T.rows; ++i) {
+        const double* tr = &T.v[static_cast<size_t>(i) * d_file];
+        double* o = &Tr.v[static_cast<size_t>(i) * d];
+        for (int k = 0; k < d_file; ++k) {
+          shift[i] += tr[k] * hull_shift[k];
+          if (tr[k] == 0.0) continue;
+          const double* brow = &hull_basis[static_cast<size_t>(k) * d];
+          for (int q = 0; q < d; ++q) o[q] += tr[k] * brow[q];
+        }
+      }
+      T = std::move(Tr);
+    }
+    Tcm = colmajor(T);
     dim = T.rows;
     prof.original_dim = T.rows;
     out.resize(static_cast<size_t>(N) * dim);
@@ -623,11 +777,13 @@ int cmd_sample_run(int argc, char** argv) {
     else if (a == "--backmap-mode") c.backmap_mode = next_arg(i, argc, argv, a);
     else if (a == "--start-policy") {
       if (next_arg(i, argc, argv, a) != "file") die_usage("invalid --start-policy (only 'file' is supported)");
-    } else if (a == "--iter-rounding-passes" || a == "--iter-rounding-warmup" || a == "--affine-hull-tol" ||
-               a == "--pair-schedule" || a == "--pair-schedule-file" || a == "--extra-constraint-eps" ||
-               a == "--constraint-eps") {
-      die_usage("unsupported flag: " + a);
-    } else die_usage("unknown flag: " + a);
+    } else if (a == "--iter-rounding-passes") c.iter_rounding_passes = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--iter-rounding-warmup") c.iter_rounding_warmup = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--pair-schedule" || a == "--pair-schedule-file") c.pair_schedule = next_arg(i, argc, argv, a);
+    else if (a == "--affine-hull-tol") c.affine_hull_tol = std::stod(next_arg(i, argc, argv, a));
+    else if (a == "--extra-constraint-eps") c.extra_constraint_eps = std::stod(next_arg(i, argc, argv, a));
+    else if (a == "--constraint-eps") c.constraint_eps = std::stod(next_arg(i, argc, argv, a));
+    else die_usage("unknown flag: " + a);
   }
   if (c.model_dir.empty()) die_usage("missing --model-dir");
   if (out_root.empty()) die_usage("missing --out-root");
@@ -637,6 +793,11 @@ int cmd_sample_run(int argc, char** argv) {
   if (c.resync_interval < 0) die_usage("invalid --resync-interval (must be >=0)");
   if (c.ksparse_prob < 0.0 || c.ksparse_prob > 1.0) die_usage("invalid --ksparse-prob (must be in [0,1])");
   if (c.ksparse_k <= 0) die_usage("invalid --ksparse-k (must be >0)");
+  if (c.iter_rounding_passes < 0) die_usage("--iter-rounding-passes must be >= 0");
+  if (c.iter_rounding_warmup < 0) die_usage("--iter-rounding-warmup must be >= 0");
+  if (c.extra_constraint_eps < 0.0) die_usage("invalid --extra-constraint-eps (must be >=0)");
+  if (c.constraint_eps < 0.0) die_usage("invalid --constraint-eps (must be >=0)");
+  if (c.affine_hull_tol < 0.0) die_usage("invalid --affine-hull-tol (must be >=0)");
   if (c.extra_constraints != "auto" && c.extra_constraints != "ignore" && c.extra_constraints != "require")
     die_usage("invalid --extra-constraints (auto|ignore|require)");
   if (c.bounds_policy != "ignore" && c.bounds_policy != "filter") die_usage("invalid --bounds-policy: " + c.bounds_policy);
@@ -680,6 +841,159 @@ int cmd_sample_run(int argc, char** argv) {
   }
   phase(st, "sampling");
   return run_sampling(c);
+}
+
+// ------------------------------------------------- calibrate-rounding
+// One pair schedule for a list of models (src/cli/sample/cmd_calibrate_rounding.cpp:24-195):
+// pairs from a shuffle seeded with --seed, then per pass one warm-up chain
+// per model (--warmup samples, thinning 1, Jacobi pairs of the schedule so
+// far, seed ^ model index ^ (pass + 1)), the pairs' population moments
+// averaged over models, and the Jacobi rotation of the averages.
+std::vector<std::string> load_model_list(const std::string& path) {
+  require_nonempty(path, "model list");
+  std::ifstream f(path);
+  if (!f.is_open()) throw std::runtime_error("cannot open model list: " + path);
+  std::vector<std::string> out;
+  for (std::string line; std::getline(f, line);) {
+    const size_t a = line.find_first_not_of(" \t\r\n"), z = line.find_last_not_of(" \t\r\n");
+    if (a == std::string::npos) continue;
+    line = line.substr(a, z - a + 1);
+    if (line[0] == '#') continue;
+    out.push_back(line);
+  }
+  if (out.empty()) throw std::runtime_error("no models in list: " + path);
+  return out;
+}
+
+int cmd_calibrate_rounding(int argc, char** argv) {
+  std::string models_root, model_list, out_csv;
+  int warmup = 2000, passes = 2, seed = 1, max_models = 0, gpu = 0;
+  double pair_prob = 0.3, extra_eps = 0.0;
+  std::string precision = "fp64", rng = "mrg";
+  for (int i = 0; i < argc; ++i) {
+    const std::string a = argv[i];
+    if (a == "--models-root") models_root = next_arg(i, argc, argv, a);
+    else if (a == "--model-list") model_list = next_arg(i, argc, argv, a);
+    else if (a == "--out") out_csv = next_arg(i, argc, argv, a);
+    else if (a == "--warmup") warmup = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--passes") passes = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--pair-prob") pair_prob = std::stod(next_arg(i, argc, argv, a));
+    else if (a == "--extra-constraint-eps") extra_eps = std::stod(next_arg(i, argc, argv, a));
+    else if (a == "--seed") seed = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--max-models") max_models = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--gpu") gpu = std::stoi(next_arg(i, argc, argv, a));
+    else if (a == "--precision") precision = next_arg(i, argc, argv, a);
+    else if (a == "--rng") rng = next_arg(i, argc, argv, a);
+    else die_usage("unknown flag: " + a);
+  }
+  if (models_root.empty()) die_usage("missing --models-root");
+  if (model_list.empty()) die_usage("missing --model-list");
+  if (out_csv.empty()) die_usage("missing --out");
+  if (warmup <= 0) die_usage("invalid --warmup");
+  if (passes <= 0) die_usage("invalid --passes");
+  if (!(pair_prob > 0.0 && pair_prob <= 1.0)) die_usage("invalid --pair-prob (0,1]");
+  if (extra_eps < 0.0) die_usage("invalid --extra-constraint-eps (must be >=0)");
+  if (max_models < 0) die_usage("invalid --max-models (must be >=0)");
+  if (precision != "fp32" && precision != "fp64") die_usage("invalid --precision (fp32|fp64)");
+  if (rng != "philox" && rng != "mrg") die_usage("invalid --rng (philox|mrg)");
+  if (seed == 0) seed = 1;
+  std::vector<std::string> names = load_model_list(model_list);
+  if (max_models > 0 && static_cast<int>(names.size()) > max_models) names.resize(max_models);
+  struct Model {
+    naja_polytope* P = nullptr;
+    std::vector<double> x0;
+  };
+  std::vector<Model> models;
+  int d = -1;
+  for (const std::string& nm : names) {
+    RunConfig c;
+    c.model_dir = absolute(models_root + "/" + nm);
+    c.model_name = nm.substr(nm.find_last_of('/') == std::string::npos ? 0 : nm.find_last_of('/') + 1);
+    c.rounding_dir = c.model_dir + "/rounding";
+    validate_contract(c);
+    Csv A = load_csv(c.file("A")), b = load_csv(c.file("b")), x0 = load_csv(c.file("start"));
+    if (path_exists(c.file("extra_A")) && path_exists(c.file("extra_b"))) {
+      Csv eA = load_csv(c.file("extra_A")), eb = load_csv(c.file("extra_b"));
+      if (eA.cols != A.cols) throw std::runtime_error("extra_A columns differ from A: " + c.file("extra_A"));
+      for (double& v : eb.v) v += extra_eps;
+      A.v.insert(A.v.end(), eA.v.begin(), eA.v.end());
+      A.rows += eA.rows;
+      b.v.insert(b.v.end(), eb.v.begin(), eb.v.end());
+    }
+    if (d < 0) d = A.cols;
+    if (A.cols != d) throw std::runtime_error("model " + nm + " has reduced dim " + std::to_string(A.cols) + ", expected " + std::to_string(d));
+    if (d < 2) throw std::runtime_error("calibrate-rounding requires reduced_dim >= 2");
+    Model mdl;
+    const std::vector<double> Acm = colmajor(A);
+    check(naja_polytope_create(gpu, A.rows, d, Acm.data(), A.rows, b.v.data(), &mdl.P));
+    mdl.x0 = x0.v;
+    models.push_back(std::move(mdl));
+  }
+  naja::rounding::PairSchedule sched = naja::rounding::random_pairing(d, static_cast<uint64_t>(seed));
+  const int np = sched.size();
+  std::vector<double> W(static_cast<size_t>(warmup) * d);
+  for (int pass = 0; pass < passes; ++pass) {
+    std::vector<double> svi(np, 0.0), svj(np, 0.0), scov(np, 0.0);
+    for (size_t mi = 0; mi < models.size(); ++mi) {
+      naja_chr_params p;
+      naja_chr_params_default(&p);
+      p.nspc = warmup;
+      p.thinning = 1;
+      p.nchains = 1;
+      p.tpb = 0;
+      p.seed = static_cast<unsigned long long>(static_cast<long long>(seed ^ static_cast<int>(mi) ^ (pass + 1)));
+      p.pair_prob = pair_prob;
+      p.pair_mode = 2;
+      p.pair_i = sched.i.data();
+      p.pair_j = sched.j.data();
+      p.pair_c = sched.c.data();
+      p.pair_s = sched.s.data();
+      p.n_pairs = np;
+      p.precision = precision == "fp64" ? NAJA_PREC_FP64 : NAJA_PREC_FP32;
+      p.rng = rng == "mrg" ? NAJA_RNG_REF_MRG : NAJA_RNG_PHILOX;
+      p.out_dtype = NAJA_DTYPE_F64;
+      check(naja_chr_run(models[mi].P, &p, models[mi].x0.data(), d, W.data(), nullptr, nullptr));
+      check(naja_polytope_check(models[mi].P));
+      for (int k = 0; k < np; ++k) {
+        const int ii = sched.i[k], jj = sched.j[k];
+        double mi_ = 0.0, mj_ = 0.0;
+        for (int t = 0; t < warmup; ++t) {
+          mi_ += W[static_cast<size_t>(t) * d + ii];
+          mj_ += W[static_cast<size_t>(t) * d + jj];
+        }
+        mi_ /= warmup;
+        mj_ /= warmup;
+        double vi = 0.0, vj = 0.0, cv = 0.0;
+        for (int t = 0; t < warmup; ++t) {
+          const double a = W[static_cast<size_t>(t) * d + ii] - mi_, bb = W[static_cast<size_t>(t) * d + jj] - mj_;
+          vi += a * a;
+          vj += bb * bb;
+          cv += a * bb;
+        }
+        svi[k] += vi / warmup;
+        svj[k] += vj / warmup;
+        scov[k] += cv / warmup;
+      }
+    }
+    const double w = static_cast<double>(models.size());
+    for (int k = 0; k < np; ++k) {
+      const auto cs = naja::rounding::jacobi_rotation_cs(svi[k] / w, svj[k] / w, scov[k] / w);
+      sched.c[k] = cs.first;
+      sched.s[k] = cs.second;
+    }
+  }
+  for (auto& mdl : models) naja_polytope_destroy(mdl.P);
+  naja::rounding::write_pair_schedule_csv(out_csv, sched);
+  std::cout << "OK\n"
+            << "out              :: " << absolute(out_csv) << "\n"
+            << "models           :: " << names.size() << "\n"
+            << "reduced_dim      :: " << d << "\n"
+            << "pairs            :: " << np << "\n"
+            << "passes           :: " << passes << "\n"
+            << "warmup           :: " << warmup << "\n"
+            << "pair_prob        :: " << pair_prob << "\n"
+            << "extra_eps        :: " << extra_eps << "\n";
+  return 0;
 }
 
 // ------------------------------------------------------------ validate
@@ -832,12 +1146,15 @@ int main(int argc, char** argv) {
   try {
     if (argc >= 3 && std::string(argv[1]) == "sample" && std::string(argv[2]) == "run")
       return cmd_sample_run(argc - 3, argv + 3);
+    if (argc >= 3 && std::string(argv[1]) == "sample" && std::string(argv[2]) == "calibrate-rounding")
+      return cmd_calibrate_rounding(argc - 3, argv + 3);
     if (argc >= 2 && std::string(argv[1]) == "validate") return cmd_validate(argc - 2, argv + 2);
     if (argc >= 2 && std::string(argv[1]) == "version") {
       std::cout << naja_version() << std::endl;
       return 0;
     }
     std::cerr << "usage:\n  naja sample run --model-dir <dir> --out-root <dir> --n-chains K --n-samples S [...]\n"
+              << "  naja sample calibrate-rounding --models-root <dir> --model-list <file> --out <csv> [...]\n"
               << "  naja validate --samples <file.npy> [--model-dir <dir>] [--n-chains 4]\n  naja version\n";
     return 2;
   } catch (const std::exception& e) {

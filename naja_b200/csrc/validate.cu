@@ -187,7 +187,7 @@ extern "C" int naja_validate(const float* samples, long long N, int dim, int nch
   const long spc = static_cast<long>(N / nchains);
   if (ess && spc < 4) return fail(NAJA_ERR_INVALID_ARGUMENT, "compute_ess: fewer than 4 samples per chain");
   if (rhat && spc / 2 < 2) return fail(NAJA_ERR_INVALID_ARGUMENT, "compute_split_rhat: chain too short to split");
-  if (spc > kEssMaxSeries)
+  if (ess && spc > kEssMaxSeries)
     return fail(NAJA_ERR_UNSUPPORTED, "naja_validate: more than " + std::to_string(kEssMaxSeries) +
                                           " samples per chain");
   if (int st = require_local("naja_validate", {samples, ess, rhat})) return st;

@@ -144,3 +144,76 @@ def diag_lowrank(log_diag, U, c, A, b) -> Rounding:
     c = np.asarray(c, dtype=np.float64)
     return Rounding(M, c.copy(), A @ M, b - A @ c, np.zeros(A.shape[1]), {"method": "diag+lowrank",
                                                                            "rank": int(U.shape[1])})
+
+
+def analytic_center(A, b, x0=None, tol: float = 1e-9, max_iter: int = 200):
+    """Analytic centre of {y : A y <= b}: argmin of -sum log(b - A y), by
+    damped Newton from a strictly feasible x0 (default 0).  Returns (x_c,
+    slack at x_c, Newton iterations)."""
+    A = np.asarray(A, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    x = np.zeros(A.shape[1]) if x0 is None else np.asarray(x0, dtype=np.float64).copy()
+    s = b - A @ x
+    if not np.all(s > 0):
+        raise ValueError("analytic_center: the start point is not strictly feasible")
+    it = 0
+    for it in range(1, max_iter + 1):
+        w = 1.0 / s
+        g = A.T @ w
+        H = (A * (w * w)[:, None]).T @ A
+        L = np.linalg.cholesky(H)
+        dx = -np.linalg.solve(L.T, np.linalg.solve(L, g))
+        lam2 = float(-g @ dx)  # Newton decrement squared
+        if lam2 <= tol * tol:
+            break
+        Adx = A @ dx
+        t = 1.0 / (1.0 + np.sqrt(lam2))  # damped step, stays inside the Dikin ellipsoid
+        pos = Adx > 0
+        if pos.any():
+            t = min(t, 0.99 * float(np.min(s[pos] / Adx[pos])))
+        x = x + t * dx
+        s = b - A @ x
+    return x, s, it
+
+
+def _sym_sqrt(S, inverse=False):
+    ev, V = np.linalg.eigh(S)
+    ev = np.maximum(ev, ev.max() * 1e-14)
+    return (V * (ev ** (-0.5 if inverse else 0.5))) @ V.T
+
+
+def dikin_full(A, b, x0=None) -> Rounding:
+    """Whole-ellipsoid Dikin rounding: y = H^{-1/2} z + x_c with x_c the
+    analytic centre and H = A^T S^-2 A its barrier Hessian (S = diag(b - A
+    x_c)).  The Dikin ellipsoid {(y - x_c)^T H (y - x_c) <= 1}, which lies
+    inside the polytope, becomes the unit ball in z, along every direction at
+    once -- where dikin() stretches at most k_directions eigen-directions by a
+    clipped factor (the reference's preconditioner)."""
+    A = np.asarray(A, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    t0 = _now()
+    x_c, s, iters = analytic_center(A, b, x0)
+    w = 1.0 / s
+    H = (A * (w * w)[:, None]).T @ A
+    M = _sym_sqrt(H, inverse=True)
+    return Rounding(M, x_c, A @ M, s.copy(), np.zeros(A.shape[1]),
+                    {"method": "dikin_full", "newton_iterations": iters, "seconds": _now() - t0})
+
+
+def from_covariance(A, b, cov, c, y0=None) -> Rounding:
+    """Rounding to the isotropic position of a sample: y = Sigma^{1/2} z + c,
+    with Sigma a sample covariance of the uniform distribution on the
+    polytope (or a factor's estimate of it).  y0 (rows of current positions,
+    optional) are carried into z so that running chains continue."""
+    A = np.asarray(A, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    M = _sym_sqrt(np.asarray(cov, dtype=np.float64))
+    c = np.asarray(c, dtype=np.float64)
+    z0 = np.zeros(A.shape[1]) if y0 is None else np.linalg.solve(M, (np.atleast_2d(y0) - c).T).T
+    return Rounding(M, c.copy(), A @ M, b - A @ c, z0, {"method": "covariance"})
+
+
+def _now():
+    import time
+
+    return time.perf_counter()

@@ -24,8 +24,10 @@ from ._lib import check, load
 from .sampler import _is_torch, _ptr, _stream_of
 
 
-def ess_rhat(samples, n_chains: int, layout: int = 1):
-    """Returns (ess[dim, n_chains], rhat[dim]) as float64 numpy arrays."""
+def ess_rhat(samples, n_chains: int, layout: int = 1, ess: bool = True, rhat: bool = True):
+    """Returns (ess[dim, n_chains], rhat[dim]) as float64 numpy arrays; a
+    metric not asked for (ess=False or rhat=False) is returned as None and
+    not computed."""
     N, dim = int(samples.shape[0]), int(samples.shape[1])
     if _is_torch(samples):
         import torch
@@ -33,11 +35,11 @@ def ess_rhat(samples, n_chains: int, layout: int = 1):
         samples = samples.to(torch.float32).contiguous()
     else:
         samples = np.ascontiguousarray(np.asarray(samples, dtype=np.float32))
-    ess = np.empty((dim, n_chains), dtype=np.float64)
-    rhat = np.empty(dim, dtype=np.float64)
-    check(load().naja_validate(_ptr(samples), N, dim, int(n_chains), int(layout), _ptr(ess), _ptr(rhat),
+    e = np.empty((dim, n_chains), dtype=np.float64) if ess else None
+    r = np.empty(dim, dtype=np.float64) if rhat else None
+    check(load().naja_validate(_ptr(samples), N, dim, int(n_chains), int(layout), _ptr(e), _ptr(r),
                                _stream_of(samples)))
-    return ess, rhat
+    return e, r
 
 
 def percentile(v, q: float) -> float:

@@ -31,3 +31,16 @@ def test_adapter_runs(cuda, tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "adapter ok" in r.stdout
+
+
+def test_rounding_header_host_logic(tmp_path):
+    """include/naja/rounding.hpp: Jacobi rotation, schedule CSV, pairing and
+    affine-hull basis (host code only; links the library, runs no kernel)."""
+    exe = tmp_path / "rounding_host"
+    cxx = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
+    cmd = [cxx, "-std=c++17", "-O1", "-I", str(ROOT / "include"), str(ROOT / "tests" / "cpp" / "rounding_host.cpp"),
+           "-o", str(exe), "-L", str(ROOT / "naja_b200"), "-lnaja_b200", f"-Wl,-rpath,{ROOT / 'naja_b200'}"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    r = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "rounding host ok" in r.stdout

@@ -102,3 +102,113 @@ def test_backmap_bounds_filter(cuda, tmp_path):
     assert rep["bounds"]["n_checked"] == 200 * 130
     # the same rule as the filter: no violating pair exactly when every sample was kept
     assert (rep["bounds"]["n_violations"] == 0) == (valid.shape[0] == 200)
+
+
+def _schedule(path, d, seed):
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(d)
+    th = rng.uniform(-np.pi, np.pi, d // 2)
+    with open(path, "w") as f:
+        f.write("# i,j,c,s\n")
+        for k in range(d // 2):
+            f.write(f"{perm[2 * k]},{perm[2 * k + 1]},{np.cos(th[k])!r},{np.sin(th[k])!r}\n")
+
+
+def test_pair_schedule_and_warmup_rounding(cuda, tmp_path):
+    """--pair-schedule and --iter-rounding-* select Jacobi-pair steps
+    (src/rounding/plan.cpp:12-62): the runs succeed, print the reference's
+    phase lines, stay feasible and differ from the run without them."""
+    md, A, b = _model_dir(tmp_path)
+    sched = tmp_path / "sched.csv"
+    _schedule(sched, 40, 1)
+    common = ["--model-dir", md, "--n-chains", 2, "--n-samples", 150, "--pair-prob", 0.4, "--resync-interval", 64,
+              "--write-npy", "--precision", "fp64"]
+    outs = {}
+    for name, extra in (("plain", []), ("file", ["--pair-schedule", sched]),
+                        ("warmup", ["--iter-rounding-passes", 2, "--iter-rounding-warmup", 300])):
+        r = _run("sample", "run", *common, "--out-root", tmp_path / name, *extra)
+        assert r.returncode == 0, r.stderr + r.stdout
+        if name == "file":
+            assert "> loading pair schedule" in r.stdout.splitlines()
+        if name == "warmup":
+            assert "> iterative rounding-lite (warmup)" in r.stdout.splitlines()
+        Y = np.load(next((tmp_path / name).iterdir()) / "samples.npy").astype(np.float64)
+        assert (Y @ A.T - b).max() <= 1e-4 * np.abs(b).max()
+        outs[name] = Y
+    assert not np.array_equal(outs["plain"], outs["file"]) and not np.array_equal(outs["plain"], outs["warmup"])
+    bad = tmp_path / "bad.csv"
+    bad.write_text("0,1,1\n")
+    r = _run("sample", "run", *common, "--out-root", tmp_path / "bad", "--pair-schedule", bad)
+    assert r.returncode == 1 and "expected 4 columns" in r.stderr
+
+
+def test_affine_hull_reduction(cuda, tmp_path):
+    """--affine-hull-tol (src/engine/job_sampling.cu:196-235, 299-303): two
+    rows tight at the start pin a plane; the chains sample inside it and the
+    composed backmap returns points of the original polytope on that plane."""
+    d = 12
+    rng = np.random.default_rng(5)
+    a = rng.standard_normal(d)
+    A = np.vstack([np.eye(d), -np.eye(d), a, -a])
+    b = np.concatenate([np.ones(d), np.ones(d), [0.0, 0.0]])
+    md = tmp_path / "models" / "H12"
+    (md / "rounding").mkdir(parents=True)
+    r_ = md / "rounding"
+    _write(r_ / "H12_rounding_A.csv", A)
+    _write(r_ / "H12_rounding_b.csv", b.reshape(-1, 1))
+    _write(r_ / "H12_rounding_start.csv", np.zeros((d, 1)))
+    _write(r_ / "H12_rounding_T.csv", np.eye(d))
+    _write(r_ / "H12_rounding_shift.csv", np.zeros((d, 1)))
+    r = _run("sample", "run", "--model-dir", md, "--out-root", tmp_path / "o1", "--n-chains", 2, "--n-samples", 300,
+             "--affine-hull-tol", 1e-9, "--write-npy", "--verbose", "--resync-interval", 100)
+    assert r.returncode == 0, r.stderr + r.stdout
+    assert "affine_hull_dim  11 (from 12)" in r.stdout
+    Z = np.load(next((tmp_path / "o1").iterdir()) / "samples.npy")
+    assert Z.shape == (600, 11)
+    r = _run("sample", "run", "--model-dir", md, "--out-root", tmp_path / "o2", "--n-chains", 2, "--n-samples", 300,
+             "--affine-hull-tol", 1e-9, "--write-npy", "--backmap", "--backmap-mode", "fp64", "--resync-interval", 100)
+    assert r.returncode == 0, r.stderr + r.stdout
+    Y = np.load(next((tmp_path / "o2").iterdir()) / "samples.npy").astype(np.float64)
+    assert Y.shape == (600, d)
+    assert np.abs(Y @ a).max() <= 1e-5  # on the plane a y = 0
+    assert (np.abs(Y).max() <= 1.0 + 1e-5) and Y.std(axis=0).min() > 0.05  # inside the box, and moving
+
+
+def test_calibrate_rounding(cuda, tmp_path):
+    """naja sample calibrate-rounding (src/cli/sample/cmd_calibrate_rounding.cpp:24-195):
+    with one pass, every pair's (c, s) is the Jacobi rotation of the pair's
+    warm-up moments averaged over the models, each model's warm-up being one
+    chain of --warmup samples with the pairs at angle 0 and seed ^ model ^ 1."""
+    root = tmp_path / "models"
+    names = []
+    for k in range(2):
+        g = synth.genome_shaped(n=120, d=30, density=0.12, seed_T=40 + k, seed_u=50 + k)
+        md = root / f"M{k}"
+        (md / "rounding").mkdir(parents=True)
+        _write(md / "rounding" / f"M{k}_rounding_A.csv", g["A"])
+        _write(md / "rounding" / f"M{k}_rounding_b.csv", g["b"].reshape(-1, 1))
+        _write(md / "rounding" / f"M{k}_rounding_start.csv", g["start"].reshape(-1, 1))
+        names.append((f"M{k}", g))
+    (tmp_path / "list.txt").write_text("# models\nM0\n\nM1\n")
+    out = tmp_path / "sched.csv"
+    r = _run("sample", "calibrate-rounding", "--models-root", root, "--model-list", tmp_path / "list.txt", "--out",
+             out, "--warmup", 400, "--passes", 1, "--pair-prob", 0.3, "--seed", 9)
+    assert r.returncode == 0, r.stderr + r.stdout
+    assert r.stdout.startswith("OK") and "pairs            :: 15" in r.stdout
+    rows = np.loadtxt(out, delimiter=",", ndmin=2)
+    i, j = rows[:, 0].astype(int), rows[:, 1].astype(int)
+    assert sorted(np.concatenate([i, j]).tolist()) == list(range(30))
+    from naja_b200 import Polytope
+
+    sv = np.zeros((3, 15))
+    for mi, (_, g) in enumerate(names):
+        P = Polytope(g["A"], g["b"])
+        W = P.run(g["start"], 400, 1, 1, seed=9 ^ mi ^ 1, pair_prob=0.3, pair_mode=2,
+                  pairs=(i, j, np.ones(15), np.zeros(15)), precision="fp64", rng="mrg", out_dtype="f64")
+        di, dj = W[:, i] - W[:, i].mean(axis=0), W[:, j] - W[:, j].mean(axis=0)
+        sv += np.stack([(di * di).mean(axis=0), (dj * dj).mean(axis=0), (di * dj).mean(axis=0)])
+    vi, vj, cij = sv / 2
+    th = 0.5 * np.arctan2(2 * cij, vi - vj)
+    want_c = np.where(cij == 0, 1.0, np.cos(th))
+    want_s = np.where(cij == 0, 0.0, np.sin(th))
+    assert np.allclose(rows[:, 2], want_c, atol=2e-5) and np.allclose(rows[:, 3], want_s, atol=2e-5)
