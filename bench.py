@@ -8,13 +8,20 @@ pair-prob 0.3, start y=0, followed by the backmap V = T y + shift of all
 200,000 samples to n=2600.  Synthetic data stands in for a rounded
 genome-scale model (none ships with the reference).
 
+The headline samples the polytope rounded by its whole Dikin ellipsoid
+(y = M z + c, M = H^-1/2 at the analytic centre; --rounding): the chains run
+in z on A M, every sample is mapped to y = M z + c (FP64 kernel) for the
+metric and to reaction space with the composed T' = T M, shift' = T c +
+shift.  The affine map leaves the uniform target unchanged.
+
 value  = chain-correct min-ESS / second of the timed job (ESS per dim summed
-         over de-interleaved chains, min over dims; seconds = sampling +
-         backmap with inputs resident in HBM), gated by split-R-hat and
-         bounds violations, which the line reports.
+         over de-interleaved chains, min over dims, in y; seconds = sampling +
+         maps with inputs resident in HBM), gated by split-R-hat and bounds
+         violations, which the line reports; `plain` repeats it without the
+         rounding, `gate_run` samples on until split-R-hat < 1.01.
 e2e    = the same min-ESS over the job run from host buffers through the C
-         ABI: polytope upload, start points, sampling, backmap, and the
-         back-transformed samples copied to pinned host memory.
+         ABI: rounding, polytope upload, sampling, backmap, and the
+         back-transformed samples copied to pinned host memory (wall clock).
 roofline: the step kernel, algorithmic bytes per CHR step
          4*m*(1+p_pair) + 4*d/thinning (one FP32 column of A per coordinate,
          two per pair step, plus the amortised sample write) over its
@@ -138,6 +145,7 @@ class Workload:
                 "n": self.n, "d": self.d, "m": self.m, "chains": self.nchains, "samples_per_chain": self.nspc,
                 "thinning": self.thin, "pair_prob": self.pair, "precision": a.precision,
                 "resync_interval": a.resync, "backmap": a.backmap_mode, "rng": "philox", "step_kernel": a.sparse,
+                "rounding": a.rounding,
                 "l2": "256 MiB buffer written between timed steps"}
 
 
@@ -169,12 +177,13 @@ def _gate(torch, W, samples_dev, ess, rhat):
             "gem_bounds_violations": int((gem > 0).sum()), "gem_bounds_checked": int(gem.numel())}
 
 
-def _backmap_error(torch, W, samples_dev, V_dev, mode):
-    """Backmap error of `mode` against an FP64 GEMM on 4096 evenly spaced samples."""
+def _backmap_error(torch, Tm, shift, samples_dev, V_dev, mode):
+    """Backmap error of `mode` against an FP64 GEMM of the same samples on
+    4096 evenly spaced ones."""
     step = max(1, samples_dev.shape[0] // 4096)
     y = samples_dev[::step].double()
-    T = torch.from_numpy(W.T).to(y.device)
-    sh = torch.from_numpy(W.shift).to(y.device)
+    T = torch.from_numpy(Tm).to(y.device)
+    sh = torch.from_numpy(shift).to(y.device)
     ref = y @ T.T + sh
     got = V_dev[::step].double()
     scale = y.abs() @ T.abs().T + sh.abs()
@@ -206,23 +215,26 @@ def _stats(v):
     return {"min": float(min(v)), "median": float(statistics.median(v)), "max": float(max(v)), "n": len(v)}
 
 
-def _cpu_baseline(W, a, min_ess_per_step):
+def _cpu_baseline(W, a, min_ess_per_step, R):
+    """The oracle on the host cores, on the polytope the headline samples
+    (rounded when it is), one thread per chain: the oracle parallelises over
+    chains, so at most `chains` threads are used whatever the host has."""
     import oracle.oracle as O
 
     cores = min(os.cpu_count() or 1, W.nchains)
     nspc = 2
     t0 = time.perf_counter()
-    O.chr_run(W.A, W.b, W.start, nspc, W.thin, W.nchains, seed=a.seed, pair_prob=W.pair, resync_interval=a.resync,
+    O.chr_run(R.A, R.b, R.z0, nspc, W.thin, W.nchains, seed=a.seed, pair_prob=W.pair, resync_interval=a.resync,
               precision=a.precision, threads=cores)
     dt = time.perf_counter() - t0
     nspc = max(2, min(W.nspc, int(nspc * a.cpu_seconds / max(dt, 1e-3))))
     t0 = time.perf_counter()
-    O.chr_run(W.A, W.b, W.start, nspc, W.thin, W.nchains, seed=a.seed, pair_prob=W.pair, resync_interval=a.resync,
+    O.chr_run(R.A, R.b, R.z0, nspc, W.thin, W.nchains, seed=a.seed, pair_prob=W.pair, resync_interval=a.resync,
               precision=a.precision, threads=cores)
     dt = time.perf_counter() - t0
     steps_s = W.nchains * nspc * W.thin / dt
     return {"value": min_ess_per_step * steps_s, "unit": UNIT, "cores": cores, "kind": "port",
-            "steps_per_s": steps_s,
+            "steps_per_s": steps_s, "host_cores": os.cpu_count(),
             "sample": f"{W.nchains} chains x {nspc} samples (thinning {W.thin}) of the same workload, CPU oracle "
                       f"{a.precision} tier, {cores} threads, {dt:.1f} s; min-ESS/s = GPU min-ESS per CHR step x "
                       f"CPU CHR steps/s (identical trajectory)"}
@@ -257,22 +269,34 @@ def _ours(a, rank, world):
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
+    from naja_b200 import gate as ng
+
     W = Workload(a)
-    P = nb.Polytope(W.A, W.b, device=dev.index)
-    T_dev = torch.from_numpy(W.T).to(dev)
-    sh_dev = torch.from_numpy(W.shift).to(dev)
-    x0 = torch.from_numpy(np.broadcast_to(W.start, (W.nchains, W.d)).copy()).to(dev)
+    # the rounding y = M z + c, the rounded polytope and the composed backmap
+    # T' = T M, shift' = T c + shift are set up once (untimed here; e2e times them)
+    R = ng.make_rounding(a.rounding, W.A, W.b, W.start)
+    rounded = R.info["method"] != "identity"
+    P = nb.Polytope(R.A, R.b, device=dev.index)
+    Tp, shp = R.compose_backmap(W.T, W.shift)
+    T_dev = torch.from_numpy(Tp).to(dev)
+    sh_dev = torch.from_numpy(shp).to(dev)
+    M_dev = torch.from_numpy(np.ascontiguousarray(R.M)).to(dev)
+    c_dev = torch.from_numpy(R.c).to(dev)
+    x0 = torch.from_numpy(np.broadcast_to(R.z0, (W.nchains, W.d)).copy()).to(dev)
     samples = torch.empty((W.nspc * W.nchains, W.d), dtype=torch.float32, device=dev)
+    zbuf = torch.empty_like(samples) if rounded else samples
     V = torch.empty((W.nspc * W.nchains, W.n), dtype=torch.float32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     seed = replica_seed(a.seed, rank)
 
     def job():
-        P.run(x0, W.nspc, W.thin, W.nchains, out=samples, seed=seed, pair_prob=W.pair,
+        P.run(x0, W.nspc, W.thin, W.nchains, out=zbuf, seed=seed, pair_prob=W.pair,
               resync_interval=a.resync, precision=a.precision, sparse=a.sparse, tpb=a.tpb)
         e_mid = torch.cuda.Event(enable_timing=True)
         e_mid.record()
-        nb.backmap(T_dev, sh_dev, samples, mode=a.backmap_mode, out=V)
+        if rounded:
+            nb.backmap(M_dev, c_dev, zbuf, mode="fp64", out=samples)  # y = M z + c for the metric
+        nb.backmap(T_dev, sh_dev, zbuf, mode=a.backmap_mode, out=V)  # v = T' z + shift'
         return e_mid
 
     for _ in range(a.warmup):
@@ -308,7 +332,7 @@ def _ours(a, rank, world):
     ms_per_step = total_ms / a.steps
     value = min_ess / (ms_per_step / 1e3)  # min-ESS already sums every rank's chains
     gate = _gate(torch, W, samples, ess, rhat)
-    bm_err = _backmap_error(torch, W, samples, V, a.backmap_mode)
+    bm_err = _backmap_error(torch, Tp, shp, zbuf, V, a.backmap_mode)
     ref_sem = nv.summary(*nv.ess_rhat(samples, W.nchains, layout=0))
     peak, peak_kind = _peaks()
     choice = P.kernel_choice(W.nspc, W.thin, W.nchains, pair_prob=W.pair, resync_interval=a.resync,
@@ -331,28 +355,34 @@ def _ours(a, rank, world):
                      "compressed_bytes_per_chr_step": W.compressed_bytes_per_step,
                      "chr_steps_per_launch": W.steps},
         "chr_steps_per_s": steps_per_s, "min_ess": min_ess,
+        "rounding": {k: v for k, v in R.info.items() if k in ("method", "newton_iterations", "seconds")},
         "job_ms": _stats(job_ms), "chr_ms": _stats(chr_ms),
         "gate": gate,
         "backmap": {"mode": a.backmap_mode, "ms": statistics.mean(bm_ms), "error_vs_fp64": bm_err,
                     "roofline": _backmap_roofline(W, statistics.mean(bm_ms), a.backmap_mode)},
         "reference_semantics_validate": {k: ref_sem[k] for k in ("status", "ess", "rhat")},
-        # per step: the CHR kernel, then the backmap (one FP64 kernel, or operand split x2 + tcgen05 GEMM)
-        "gpu_launches": a.steps * (1 + (1 if a.backmap_mode == "fp64" else 3)),
+        # per step: the CHR kernel, the y map (one FP64 kernel) when rounded, then the backmap
+        # (one FP64 kernel, or operand split x2 + tcgen05 GEMM)
+        "gpu_launches": a.steps * (1 + (1 if rounded else 0) + (1 if a.backmap_mode == "fp64" else 3)),
     }
     line["clocks"] = clk.summary()
     detail = {"job_ms": job_ms, "chr_ms": chr_ms, "backmap_ms": bm_ms}
+    if rank == 0 and rounded:
+        line["plain"] = _plain_figure(a, W, torch, dev)
     if rank == 0 and a.fp64_figure:
-        line["fp64_tier"] = _fp64_figure(a, W, P, x0, torch, dev)
+        line["fp64_tier"] = _fp64_figure(a, W, P, x0, torch, dev, M_dev, c_dev, T_dev, sh_dev)
     if rank == 0 and a.cube:
         line["unit_cube"] = _unit_cube(a, torch, dev)
     if a.e2e and rank == 0:
         line["e2e"] = _e2e(a, W, torch, dev, min_ess)
     if rank == 0 and world == 1 and not a.no_cpu:
-        line["cpu_baseline"] = _cpu_baseline(W, a, min_ess / W.steps)
+        line["cpu_baseline"] = _cpu_baseline(W, a, min_ess / W.steps, R)
     if rank == 0 and a.batch_models > 0:
         line["batched"] = _batched(a, torch, dev)
     if rank == 0 and a.gate_budget_s > 0:
-        line["gate_run"] = _gate(a)
+        line["gate_run"] = _gate_run(a)
+    if rank == 0 and a.precision_figures:
+        line["precision_study"] = _precision_study(a)
     if rank == 0 and a.learned_train > 0:
         line["learned_rounding"], detail["learned_rounding"] = _learned(a)
     if rank == 0 and a.detail_file:
@@ -363,31 +393,83 @@ def _ours(a, rank, world):
 
 
 def _e2e(a, W, torch, dev, min_ess):
+    """The same job from host buffers through the public API, wall-clock per
+    job: the rounding (host FP64: analytic centre, barrier Hessian, its
+    inverse square root, A M and T M), the rounded polytope's upload, then
+    sampling, backmap and the copy of every back-mapped sample to pinned
+    host memory overlapped chunk by chunk (naja_chr_run_backmapped)."""
     import naja_b200 as nb
+    from naja_b200 import gate as ng
     from naja_b200.pipeline import sample_backmapped
 
     pinned_out = torch.empty((W.nspc * W.nchains, W.n), dtype=torch.float32, pin_memory=True)
-    x0 = np.ascontiguousarray(np.broadcast_to(W.start, (W.nchains, W.d)))
-    h2d = W.A.nbytes + W.b.nbytes + x0.nbytes + W.T.nbytes + W.shift.nbytes
-    d2h = pinned_out.numel() * 4
-    times = []
+    times, h2d = [], 0
     for k in range(a.warmup + a.steps):
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        P = nb.Polytope(W.A, W.b, device=dev.index)
+        t0 = time.perf_counter()
+        R = ng.make_rounding(a.rounding, W.A, W.b, W.start)
+        Tp, shp = R.compose_backmap(W.T, W.shift)
+        z0 = np.ascontiguousarray(np.broadcast_to(R.z0, (W.nchains, W.d)))
+        P = nb.Polytope(R.A, R.b, device=dev.index)
         # sampling, backmap and copy to host overlapped chunk by chunk (same samples as one launch)
-        sample_backmapped(P, W.T, W.shift, x0, W.nspc, W.thin, W.nchains, pinned_out, mode=a.backmap_mode,
+        sample_backmapped(P, Tp, shp, z0, W.nspc, W.thin, W.nchains, pinned_out, mode=a.backmap_mode,
                           seed=a.seed, pair_prob=W.pair, resync_interval=a.resync, precision=a.precision,
                           sparse=a.sparse, tpb=a.tpb)
-        e1.record()
         torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
         P.close()
+        h2d = R.A.nbytes + R.b.nbytes + z0.nbytes + Tp.nbytes + shp.nbytes
         if k >= a.warmup:
-            times.append(e0.elapsed_time(e1))
+            times.append(dt * 1e3)
     ms = statistics.mean(times)
-    return {"value": min_ess / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "ms_per_step": ms}
+    return {"value": min_ess / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(pinned_out.numel() * 4), "ms_per_step": ms,
+            "timing": "wall clock per job with a device synchronise on both sides; rounding computed on the host "
+                      "inside the timed region"}
+
+
+def _plain_figure(a, W, torch, dev):
+    """The same job without rounding (plain CHR on the polytope as given,
+    the compressed-column kernel): min-ESS/s of the last of two timed jobs
+    and that kernel's roofline."""
+    import naja_b200 as nb
+    from naja_b200 import validate as nv
+
+    P = nb.Polytope(W.A, W.b, device=dev.index)
+    x0 = torch.from_numpy(np.broadcast_to(W.start, (W.nchains, W.d)).copy()).to(dev)
+    samples = torch.empty((W.nspc * W.nchains, W.d), dtype=torch.float32, device=dev)
+    V = torch.empty((W.nspc * W.nchains, W.n), dtype=torch.float32, device=dev)
+    T_dev = torch.from_numpy(W.T).to(dev)
+    sh_dev = torch.from_numpy(W.shift).to(dev)
+    chr_ms, job_ms = [], []
+    for k in range(3):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        P.run(x0, W.nspc, W.thin, W.nchains, out=samples, seed=a.seed, pair_prob=W.pair, resync_interval=a.resync,
+              precision=a.precision, sparse=a.sparse, tpb=a.tpb)
+        e1.record()
+        nb.backmap(T_dev, sh_dev, samples, mode=a.backmap_mode, out=V)
+        e2.record()
+        torch.cuda.synchronize()
+        if k:
+            chr_ms.append(e0.elapsed_time(e1))
+            job_ms.append(e0.elapsed_time(e2))
+    P.check()
+    ess, rhat = nv.ess_rhat(samples, W.nchains, layout=1)
+    min_ess = float(ess.sum(axis=1).min())
+    choice = P.kernel_choice(W.nspc, W.thin, W.nchains, pair_prob=W.pair, resync_interval=a.resync,
+                             precision=a.precision, sparse=a.sparse, tpb=a.tpb)
+    peak, peak_kind = _peaks()
+    cm = statistics.mean(chr_ms)
+    ach = W.bytes_per_step * W.steps / (cm / 1e3) / 1e9
+    P.close()
+    return {"value": min_ess / (statistics.mean(job_ms) / 1e3), "unit": UNIT, "min_ess": min_ess,
+            "rhat_max": float(rhat.max()), "ms_per_job": statistics.mean(job_ms), "chr_ms": cm,
+            "chr_steps_per_s": W.steps / (cm / 1e3),
+            "roofline": {"kernel": "chr_sparse_kernel" if choice["kernel"] == "columns" else "chr_kernel",
+                         "threads": choice["threads"], "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "peak_source": peak_kind,
+                         "compressed_bytes_per_chr_step": W.compressed_bytes_per_step}}
 
 
 def _batched(a, torch, dev):
@@ -448,7 +530,7 @@ def _batched(a, torch, dev):
                                    key=lambda r: -r["M_steps_per_s"])[:5]}
 
 
-def _gate(a):
+def _gate_run(a):
     """The metric at its gate: the genome-shaped workload's 16 chains
     (thinning 116, pair-prob 0.3, resync 2048, FP32 tier, Philox seed 0)
     continued chunk by chunk (12,500 samples per chain per chunk) until
@@ -478,15 +560,20 @@ def _gate(a):
 
 
 def _precision_study(a):
-    """FP32 tier with FP64 recompute every K steps against the FP64 tier, and
-    the split-precision backmap against FP64, on the genome-shaped polytope at
-    d=1500, n=7000 (m=14000): 8 chains x 200 samples, thinning 250,
-    pair-prob 0.3, identical Philox streams for every run.  Per run: kernel
-    time, polytope bound violations (A y <= b + 1e-6 max(1,|b|)), and the
-    position divergence from the FP64 run (max and RMS over all saved
-    coordinates, relative to the coordinate's range in the FP64 run).  Backmap:
-    max / RMS relative error over 20,000 samples (|v| > 1e-3 max|v|) and the
-    time of 200,000 samples per mode."""
+    """FP32 tier with its FP64 slack recompute every K steps against the FP64
+    tier, and the split-precision backmap against FP64, on the genome-shaped
+    polytope at d=1500, n=7000 (m=14000): 8 chains x 200 samples, thinning
+    256 (51,200 steps, a multiple of every K), pair-prob 0.3, identical
+    Philox streams for every run.  Per run: kernel time, polytope bound
+    violations (A y <= b + 1e-6 max(1,|b|)); the slack drift after the last
+    K steps, |slack32 - (b - A x)| in FP64 at the final state (max, RMS, max
+    relative to max(1, |b|)); the position divergence from the FP64 run (max
+    and RMS over all saved coordinates relative to the coordinate's range in
+    the FP64 run) and the horizon over which positions agree (steps before a
+    chain's first saved sample that differs by more than 1e-3 of a
+    coordinate's range: minimum and median over chains).  Backmap: max / RMS
+    relative error over 20,000 samples (|v| > 1e-3 max|v|) and the time of
+    200,000 samples per mode."""
     import torch
 
     from naja_b200 import Polytope, backmap, synth
@@ -495,33 +582,47 @@ def _precision_study(a):
     A, b = g["A"], g["b"]
     dev = torch.device("cuda:0")
     P = Polytope(A, b)
-    nch, nspc, thin = 8, 200, 250
-    X0 = np.zeros((nch, 1500))
+    nch, nspc, thin, d = 8, 200, 256, 1500
+    X0 = np.zeros((nch, d))
     At = torch.from_numpy(A).to(dev)
     bt = torch.from_numpy(b).to(dev)
     tol = 1e-6 * torch.clamp(bt.abs(), min=1.0)
 
     def run(precision, K):
         P.run(X0, 2, thin, nch, seed=a.seed, pair_prob=0.3, precision=precision, resync_interval=K)  # warm
-        out = torch.empty((nspc * nch, 1500), dtype=torch.float64, device=dev)
+        out = torch.empty((nspc * nch, d), dtype=torch.float64, device=dev)
+        xf = torch.empty((nch, d), dtype=torch.float64, device=dev)
+        sf = torch.empty((nch, A.shape[0]), dtype=torch.float64 if precision == "fp64" else torch.float32,
+                         device=dev)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         P.run(X0, nspc, thin, nch, seed=a.seed, pair_prob=0.3, precision=precision, resync_interval=K, out=out,
-              out_dtype="f64")
+              out_dtype="f64", X_final=xf, slack_final=sf)
         e1.record()
         torch.cuda.synchronize()
+        P.check()
         r = out @ At.T - bt
-        return out, e0.elapsed_time(e1), int((r > tol).sum()), float(r.max())
+        exact = bt - xf @ At.T
+        drift = (sf.double() - exact).abs()
+        return out, e0.elapsed_time(e1), int((r > tol).sum()), float(r.max()), {
+            "max": float(drift.max()), "rms": float(drift.pow(2).mean().sqrt()),
+            "max_rel": float((drift / torch.clamp(bt.abs(), min=1.0)).max())}
 
-    ref, t64, v64, w64 = run("fp64", 0)
+    ref, t64, v64, w64, dr64 = run("fp64", 0)
     span = (ref.max(dim=0).values - ref.min(dim=0).values).clamp(min=1e-12)
-    rows = [{"tier": "fp64", "K": 0, "ms": t64, "bound_violations": v64, "worst_violation": w64}]
+    rows = [{"tier": "fp64", "K": 0, "ms": t64, "bound_violations": v64, "worst_violation": w64,
+             "slack_drift": dr64}]
     for K in (0, 1024, 256, 64):
-        y, t, v, w = run("fp32", K)
+        y, t, v, w, dr = run("fp32", K)
         rel = (y - ref).abs() / span
+        per_sample = rel.view(nspc, nch, d).amax(dim=2)  # (sample, chain)
+        off = (per_sample > 1e-3).cpu().numpy()
+        first = np.where(off.any(axis=0), off.argmax(axis=0), nspc)  # first diverging saved sample per chain
+        horizon = first * thin
         rows.append({"tier": "fp32", "K": K, "ms": t, "time_vs_fp64": t / t64, "bound_violations": v,
-                     "worst_violation": w, "divergence_max": float(rel.max()),
-                     "divergence_rms": float(rel.pow(2).mean().sqrt())})
+                     "worst_violation": w, "slack_drift": dr, "divergence_max": float(rel.max()),
+                     "divergence_rms": float(rel.pow(2).mean().sqrt()),
+                     "agree_1e-3_steps_min": int(horizon.min()), "agree_1e-3_steps_median": float(np.median(horizon))})
     T = torch.from_numpy(g["T"]).to(dev)
     sh = torch.from_numpy(g["shift"]).to(dev)
     Y = ref.float()
@@ -535,17 +636,18 @@ def _precision_study(a):
         backmap(g["T"], g["shift"], ysub, mode=mode, out=V)
         rel = ((V.double() - vref).abs()[nz] / vref.abs()[nz])
         Vb = torch.empty((200000, 7000), dtype=torch.float32, device=dev)
-        backmap(g["T"], g["shift"], Ybig, mode=mode, out=Vb)  # warm
+        backmap(T, sh, Ybig, mode=mode, out=Vb)  # warm
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        backmap(g["T"], g["shift"], Ybig, mode=mode, out=Vb)
+        backmap(T, sh, Ybig, mode=mode, out=Vb)
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         bm[mode] = {"max_rel": float(rel.max()), "rms_rel": float(rel.pow(2).mean().sqrt()), "ms_200k": ms,
                     "tflops": 2.0 * 7000 * 1500 * 200000 / (ms / 1e3) / 1e12}
         del V, Vb
-    return {"workload": "genome-shaped n=7000 d=1500 m=14000, 8 chains x 200 samples, thinning 250, pair 0.3",
+    P.close()
+    return {"workload": "genome-shaped n=7000 d=1500 m=14000, 8 chains x 200 samples, thinning 256, pair 0.3",
             "chr": rows, "backmap": bm}
 
 
@@ -573,24 +675,24 @@ def _strip_lists(obj):
     return obj
 
 
-def _fp64_figure(a, W, P, x0, torch, dev):
+def _fp64_figure(a, W, P, x0, torch, dev, M_dev, c_dev, T_dev, sh_dev):
     """The same job in the FP64 tier (the reference's arithmetic): FP64 A,
     slack, ratios and alpha, samples written as float.  Two timed jobs after
     one warm-up; min-ESS/s of the last job, sampling + backmap time."""
     from naja_b200 import backmap
     from naja_b200 import validate as nv
 
-    samples = torch.empty((W.nspc * W.nchains, W.d), dtype=torch.float32, device=dev)
+    z = torch.empty((W.nspc * W.nchains, W.d), dtype=torch.float32, device=dev)
+    samples = torch.empty_like(z)
     V = torch.empty((W.nspc * W.nchains, W.n), dtype=torch.float32, device=dev)
-    T_dev = torch.from_numpy(W.T).to(dev)
-    sh_dev = torch.from_numpy(W.shift).to(dev)
     times = []
     for k in range(3):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        P.run(x0, W.nspc, W.thin, W.nchains, out=samples, seed=a.seed, pair_prob=W.pair, resync_interval=0,
+        P.run(x0, W.nspc, W.thin, W.nchains, out=z, seed=a.seed, pair_prob=W.pair, resync_interval=0,
               precision="fp64", sparse=a.sparse)
-        backmap(T_dev, sh_dev, samples, mode=a.backmap_mode, out=V)
+        backmap(M_dev, c_dev, z, mode="fp64", out=samples)
+        backmap(T_dev, sh_dev, z, mode=a.backmap_mode, out=V)
         e1.record()
         torch.cuda.synchronize()
         if k:
@@ -739,6 +841,9 @@ def main(argv=None):
     ap.add_argument("--sparse", default="auto", choices=["auto", "dense", "columns"],
                     help="step kernel: compressed columns, dense, or the library's automatic choice")
     ap.add_argument("--backmap-mode", default="tf32x3", choices=["fp64", "bf16x3", "tf32x3"])
+    ap.add_argument("--rounding", default="dikin_full", choices=["none", "dikin", "dikin_full"],
+                    help="rounding of the headline job: whole-ellipsoid Dikin (default), the reference's "
+                         "Dikin preconditioner, or none (plain CHR)")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -759,6 +864,8 @@ def main(argv=None):
                     help="run-to-gate section: seconds per rounding method (0 = skip)")
     ap.add_argument("--detail-file", default="",
                     help="write per-step times and per-variant records here (JSON)")
+    ap.add_argument("--no-precision-study", dest="precision_figures", action="store_false",
+                    help="skip the FP32/FP64 tier and backmap precision section")
     ap.add_argument("--precision-study", action="store_true",
                     help="run only the FP32/FP64 tier and backmap precision study and print it")
     a = ap.parse_args(argv)

@@ -91,6 +91,11 @@ typedef struct naja_chr_params {
                               takes ksparse_prob = 0 and cluster <= 1, and tpb 0 (automatic), 32, 64,
                               128, 256 or 512 when forced (automatic selection needs tpb 0); results
                               are identical for every value */
+    void* slack_final;     /* nullable, host or device: each chain's slack b - A x after its last step,
+                              nchains x m values (FP32 tier: float, FP64 tier: double), chain-major;
+                              one CTA per chain only.  The FP32 tier's drift from the exact slack is
+                              this minus b - A x_final in FP64 (the reference's resync hook,
+                              src/gpu/chr.cu:384-395, bounds it every resync_interval steps) */
 } naja_chr_params;
 
 /* Fills `p` with the reference's defaults (gpusamplers.h:30-46): tpb auto,

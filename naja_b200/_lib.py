@@ -116,6 +116,7 @@ class ChrParams(C.Structure):
         ("wait_cycles", C.c_void_p),
         ("cluster", C.c_int),
         ("sparse", C.c_int),
+        ("slack_final", C.c_void_p),
     ]
 
 

@@ -555,7 +555,7 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
   DeviceGuard g(P->device);
   if (!g.ok()) return fail(NAJA_ERR_CUDA, "naja_chr_run: cannot select device");
   if (int st = require_local("CoordinateHitAndRun", {X0, samples, X_final, p->pair_i, p->pair_j, p->pair_c,
-                                                      p->pair_s, p->rng_state, p->wait_cycles}))
+                                                      p->pair_s, p->rng_state, p->wait_cycles, p->slack_final}))
     return st;
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
 
@@ -570,7 +570,7 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
   const size_t out_bytes = static_cast<size_t>(p->nspc) * out_nchains * d * out_elt;
   const size_t x_bytes = static_cast<size_t>(ldx) * (p->nchains - 1) * sizeof(double) + d * sizeof(double);
 
-  DeviceBuffer bx0, bout, bxf, bpi, bpj, bpc, bps;
+  DeviceBuffer bx0, bout, bxf, bpi, bpj, bpc, bps, bsf;
   const void* dX0 = nullptr;
   if ((st = device_view(X0, x_bytes, stream, bx0, &dX0))) return st;
   void* dout = samples;
@@ -589,6 +589,15 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
   if (host_xf) {
     if ((st = bxf.alloc(x_bytes, stream))) return st;
     dxf = static_cast<double*>(bxf.ptr);
+  }
+  if (p->slack_final && cfg.cluster > 1)
+    return fail(NAJA_ERR_UNSUPPORTED, "CoordinateHitAndRun: slack_final needs one CTA per chain (cluster <= 1)");
+  const size_t sf_bytes = static_cast<size_t>(p->nchains) * P->m * (p->precision == NAJA_PREC_FP64 ? 8 : 4);
+  void* dsf = p->slack_final;
+  const bool host_sf = p->slack_final && !is_device_ptr(p->slack_final);
+  if (host_sf) {
+    if ((st = bsf.alloc(sf_bytes, stream))) return st;
+    dsf = bsf.ptr;
   }
   const void *dpi = nullptr, *dpj = nullptr, *dpc = nullptr, *dps = nullptr;
   if (p->n_pairs > 0) {
@@ -633,6 +642,7 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
   a.err = P->err;
   a.timeout_ns = kWaitTimeoutNs;
   a.wait_cycles = p->wait_cycles;
+  a.slack_final = dsf;
 
   st = use_sparse ? chr_sparse_launch(p->precision, a, spa, p->nchains, cfg, stream)
                   : chr_launch(p->precision, a, p->nchains, cfg, stream);
@@ -640,10 +650,11 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
     cudaError_t e = cudaGetLastError();
     return fail(st, std::string("CoordinateHitAndRun: launch failed: ") + cudaGetErrorString(e));
   }
-  if (host_out || host_xf) {
+  if (host_out || host_xf || host_sf) {
     cudaError_t e = cudaSuccess;
     if (host_out) e = cudaMemcpyAsync(samples, dout, out_bytes, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess && host_xf) e = cudaMemcpyAsync(X_final, dxf, x_bytes, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess && host_sf) e = cudaMemcpyAsync(p->slack_final, dsf, sf_bytes, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return fail(NAJA_ERR_CUDA, std::string("CoordinateHitAndRun: ") + cudaGetErrorString(e));
     if ((st = read_device_error(P->err))) return st;

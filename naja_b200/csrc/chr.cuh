@@ -43,6 +43,9 @@ struct ChrArgs {
   // staged columns, producer cycles waiting for free slots, consumer cycles
   // in the step loop, producer cycles in its loop.
   unsigned long long* wait_cycles;
+  // Nullable: receives each chain's slack b - A x after its last step
+  // (nchains x m values of the tier's type, chain-major).
+  void* slack_final;
 };
 
 struct ChrLaunchConfig {

@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(NT + 32, NT >= 512 ? 2 : (NT == 256 ? 3 : 4))
       a.chain_base = 0;
       a.rng_state = nullptr;
       a.wait_cycles = nullptr;
+      a.slack_final = nullptr;
       item_args = a;
     }
     __syncthreads();

@@ -1007,6 +1007,36 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
   if (a.X_final) {
     for (int j = tid; j < d; j += NT) a.X_final[static_cast<size_t>(chain_local) * a.ldx + j] = xs[j];
   }
+  if (a.slack_final) {
+    // the last step's pending update first (the fused order defers it)
+    Real* so = static_cast<Real*>(a.slack_final) + static_cast<size_t>(chain_local) * m;
+    for_chunks(
+        [&](int k, int base) {
+          Real s[V];
+          slack_get(k, base, s);
+          if constexpr (FUSED) {
+            if (pending) {
+#pragma unroll
+              for (int v = 0; v < V; ++v) s[v] = T::slack_update(s[v], alpha_prev, ae_prev[k * V + v]);
+            }
+          }
+#pragma unroll
+          for (int v = 0; v < V; ++v) so[base + v] = s[v];
+        },
+        [&](int base) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) {
+            const int r = base + v;
+            if (r < m) {
+              Real sv = slack_tail(r);
+              if constexpr (FUSED) {
+                if (pending) sv = T::slack_update(sv, alpha_prev, ae_prev_tail[v]);
+              }
+              so[r] = sv;
+            }
+          }
+        });
+  }
   if (TIMING && a.wait_cycles && tid == 0) {
     a.wait_cycles[4 * chain_local + 0] = w_full;
     a.wait_cycles[4 * chain_local + 2] = clock64() - c_start;
@@ -1081,6 +1111,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
       a.samples = nullptr;
       a.X_final = nullptr;
       a.wait_cycles = nullptr;
+      a.slack_final = nullptr;
     }
     slice = a;
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.full_off);

@@ -391,6 +391,11 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
   if (a.X_final) {
     for (int j = tid; j < d; j += NT) a.X_final[static_cast<size_t>(chain_local) * a.ldx + j] = xs[j];
   }
+  if (a.slack_final) {
+    consumers_sync<NW>(1);  // every thread's last slack writes are visible
+    Real* so = static_cast<Real*>(a.slack_final) + static_cast<size_t>(chain_local) * m;
+    for (int r = tid; r < m; r += NT) so[r] = slack[r];
+  }
   if (a.wait_cycles && tid == 0) {
     a.wait_cycles[4 * chain_local + 0] = w_full;
     a.wait_cycles[4 * chain_local + 2] = clock64() - c_start;
@@ -499,6 +504,7 @@ __global__ void __launch_bounds__(NW * 32 + 32, NW >= 8 ? 2 : (NW == 4 ? 3 : 4))
       a.chain_base = 0;
       a.rng_state = nullptr;
       a.wait_cycles = nullptr;
+      a.slack_final = nullptr;
       item_args = a;
       item_sp = md.sp;
     }

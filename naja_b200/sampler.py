@@ -106,7 +106,7 @@ class Polytope:
     def params(self, nspc, thinning, nchains, *, tpb=-1, seed=0, pair_prob=0.0, resync_interval=0,
                ksparse_prob=0.0, ksparse_k=8, pair_mode=1, pairs=None, precision="fp32", rng="philox",
                out_dtype="f32", chain_base=0, out_nchains=0, step_offset=0, max_slots=0, rng_state=None,
-               wait_cycles=None, cluster=0, sparse="auto"):
+               wait_cycles=None, cluster=0, sparse="auto", slack_final=None):
         p = ChrParams()
         load().naja_chr_params_default(C.byref(p))
         p.nspc, p.thinning, p.nchains, p.tpb = int(nspc), int(thinning), int(nchains), int(tpb)
@@ -136,6 +136,8 @@ class Polytope:
             p.wait_cycles = _ptr(wait_cycles).value
         p.cluster = int(cluster)
         p.sparse = _SPARSE[sparse]
+        if slack_final is not None:
+            p.slack_final = _ptr(slack_final).value
         return p, keep
 
     def kernel_choice(self, nspc, thinning, nchains, **kw):

@@ -51,7 +51,8 @@ def test_params_struct_layout():
     P = _lib.ChrParams
     assert P.seed.offset == 16 and P.pair_prob.offset == 24 and P.ksparse_prob.offset == 40
     assert P.pair_i.offset == 56 and P.n_pairs.offset == 88 and P.step_offset.offset == 112
-    assert P.cluster.offset == 144 and P.sparse.offset == 148 and C.sizeof(P) == 152
+    assert P.cluster.offset == 144 and P.sparse.offset == 148 and P.slack_final.offset == 152
+    assert C.sizeof(P) == 160
 
 
 def test_version_string():

@@ -111,7 +111,7 @@ def _schedule(path, d, seed):
     with open(path, "w") as f:
         f.write("# i,j,c,s\n")
         for k in range(d // 2):
-            f.write(f"{perm[2 * k]},{perm[2 * k + 1]},{np.cos(th[k])!r},{np.sin(th[k])!r}\n")
+            f.write(f"{perm[2 * k]},{perm[2 * k + 1]},{float(np.cos(th[k]))!r},{float(np.sin(th[k]))!r}\n")
 
 
 def test_pair_schedule_and_warmup_rounding(cuda, tmp_path):
