@@ -535,18 +535,16 @@ def _gate_run(a):
     (thinning 116, pair-prob 0.3, resync 2048, FP32 tier, Philox seed 0)
     continued chunk by chunk (12,500 samples per chain per chunk) until
     split-R-hat < 1.01 with no bound violations, or until the time budget;
-    per rounding: plain (none), the reference's Dikin preconditioner, the
-    whole-ellipsoid Dikin rounding, and the latter refined once to the
-    samples' isotropic position after two warm-up chunks.  Seconds include
-    computing the rounding, every chunk's sampling and back-map to y, and the
-    R-hat checks; min-ESS is over the samples that count (after the warm-up)."""
+    per rounding: plain (none), the reference's Dikin preconditioner and the
+    whole-ellipsoid Dikin rounding.  Seconds include computing the rounding,
+    every chunk's sampling and back-map to y, and the R-hat checks."""
     from naja_b200 import gate, synth
 
     g = synth.genome_shaped(n=a.n, d=a.d, density=0.08, seed_T=0, seed_u=1)
     out = {"workload": f"genome-shaped n={a.n} d={a.d}, {a.nchains} chains, chunks of {a.nspc} samples x thinning "
                        f"{a.thinning}, pair-prob {a.pair_prob}, until split-R-hat < 1.01 or {a.gate_budget_s:.0f} s",
            "methods": {}}
-    for method, adapt in (("none", 0), ("dikin", 0), ("dikin_full", 0), ("dikin_full", 2)):
+    for method, adapt in (("none", 0), ("dikin", 0), ("dikin_full", 0)):
         r = gate.sample_to_gate(g["A"], g["b"], g["start"], method=method, adapt_after=adapt, nchains=a.nchains,
                                 thinning=a.thinning, chunk_nspc=a.nspc, pair_prob=a.pair_prob,
                                 resync_interval=a.resync, seed=a.seed, budget_s=a.gate_budget_s)
@@ -652,19 +650,22 @@ def _precision_study(a):
 
 
 def _learned(a):
-    """Learned vs Dikin vs plain CHR on held-out conditioned variants of the
-    genome-shaped polytope (the batched-variant generator): the rounding
-    network is trained on the project's kernels from covariance factors of
-    plain-CHR samples of the training variants (training time reported
-    separately); each method then samples the held-out variants in one
-    batched launch, 8 chains x 1000 samples, thinning 116, pair-prob 0.3;
-    min-ESS (chain-summed, y-space) per variant over its share of the
-    sampling + rounding-map time."""
+    """Learned rounding on conditioned variants of the genome-shaped polytope
+    (the batched-variant generator): the network, trained on the project's
+    kernels from plain-CHR sample covariances of the training variants in
+    the base model's rounded coordinates (training time reported
+    separately), predicts each held-out variant's rounding; every method
+    (plain, the reference's Dikin, whole-ellipsoid Dikin per variant, the
+    base rounding alone, learned) then samples all held-out variants in
+    batched launches, 8 chains each, thinning 116, pair-prob 0.3, until
+    split-R-hat < 1.01 or the budget; min-ESS (chain-summed, y-space) per
+    variant over its share of the batch time plus its rounding time."""
     from naja_b200 import learned
 
     full = learned.run_experiment(n=a.n, d=a.d, n_train=a.learned_train, n_test=a.learned_test,
-                                  nchains=8, nspc_train=500, nspc_test=1000, thinning=a.thinning,
-                                  pair_prob=a.pair_prob, epochs=a.learned_epochs, resync=a.resync, seed=a.seed)
+                                  nchains=8, nspc_train=a.learned_nspc, thinning=a.thinning,
+                                  pair_prob=a.pair_prob, epochs=a.learned_epochs, resync=a.resync, seed=a.seed,
+                                  gate_budget_s=a.learned_budget_s)
     return _strip_lists(full), full
 
 
@@ -853,9 +854,12 @@ def main(argv=None):
     ap.add_argument("--batch-shape", default="", help="threads,slots,slack_smem,ctas_per_sm[,sparse] (skips the autotuner)")
     ap.add_argument("--ref-cpu", action="store_true", help="reference arm: time the CPU restatement")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
-    ap.add_argument("--learned-train", type=int, default=256,
+    ap.add_argument("--learned-train", type=int, default=1024,
                     help="learned-rounding section: training variants (0 = skip)")
     ap.add_argument("--learned-test", type=int, default=16)
+    ap.add_argument("--learned-nspc", type=int, default=1500, help="samples per chain of each training variant")
+    ap.add_argument("--learned-budget-s", type=float, default=45.0,
+                    help="learned-rounding section: seconds per method of the held-out run to the gate")
     ap.add_argument("--learned-epochs", type=int, default=60)
     ap.add_argument("--no-fp64-figure", dest="fp64_figure", action="store_false",
                     help="skip the FP64-tier figure of the same job")

@@ -161,12 +161,15 @@ typedef struct naja_batch_config {
  * and its chains are numbered 0..nchains-1, so it draws exactly the streams a
  * standalone naja_chr_run of that model with that seed draws.  X0s[k]
  * (d x nchains, leading dimension ldx) and samples[k] ((nspc*nchains) x d,
- * params->out_dtype) are device pointers.  FP32 tier.  This replaces the
- * reference's model-by-model bulk loop (src/engine/job_bulk.cpp:115-189),
- * which launches one small CoordinateHitAndRun per model. */
+ * params->out_dtype) are device pointers; X_finals (nullable array, entries
+ * nullable) receives each model's last states like naja_chr_run's X_final, so
+ * a later launch with params->step_offset continues the chains.  FP32 tier.
+ * This replaces the reference's model-by-model bulk loop
+ * (src/engine/job_bulk.cpp:115-189), which launches one small
+ * CoordinateHitAndRun per model. */
 int naja_chr_run_batched(int nmodels, const naja_polytope* const* models, const naja_chr_params* params,
-                         const double* const* X0s, int ldx, void* const* samples, unsigned long long seed_stride,
-                         const naja_batch_config* config, void* stream);
+                         const double* const* X0s, int ldx, void* const* samples, double* const* X_finals,
+                         unsigned long long seed_stride, const naja_batch_config* config, void* stream);
 /* Resident chains per SM that `config` allows for these models (0 if none). */
 int naja_batch_occupancy(int nmodels, const naja_polytope* const* models, const naja_batch_config* config,
                          int* ctas_per_sm);
@@ -175,7 +178,7 @@ int naja_batch_occupancy(int nmodels, const naja_polytope* const* models, const 
  * with naja_graph_launch, check it with naja_graph_check, release it with
  * naja_graph_destroy. */
 int naja_chr_capture_batched(int nmodels, const naja_polytope* const* models, const naja_chr_params* params,
-                             const double* const* X0s, int ldx, void* const* samples,
+                             const double* const* X0s, int ldx, void* const* samples, double* const* X_finals,
                              unsigned long long seed_stride, const naja_batch_config* config, void** graph);
 int naja_graph_launch(void* graph, void* stream);
 int naja_graph_check(void* graph);

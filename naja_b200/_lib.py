@@ -173,9 +173,9 @@ def load() -> C.CDLL:
     lib.naja_mrg_init_states.argtypes = [i, ull, i, i, vp]
     lib.naja_version.restype = C.c_char_p
     pp = C.POINTER(C.c_void_p)
-    lib.naja_chr_run_batched.argtypes = [i, pp, C.POINTER(ChrParams), pp, i, pp, ull, C.POINTER(BatchConfig), vp]
+    lib.naja_chr_run_batched.argtypes = [i, pp, C.POINTER(ChrParams), pp, i, pp, vp, ull, C.POINTER(BatchConfig), vp]
     lib.naja_batch_occupancy.argtypes = [i, pp, C.POINTER(BatchConfig), C.POINTER(i)]
-    lib.naja_chr_capture_batched.argtypes = [i, pp, C.POINTER(ChrParams), pp, i, pp, ull, C.POINTER(BatchConfig),
+    lib.naja_chr_capture_batched.argtypes = [i, pp, C.POINTER(ChrParams), pp, i, pp, vp, ull, C.POINTER(BatchConfig),
                                              C.POINTER(vp)]
     lib.naja_graph_launch.argtypes = [vp, vp]
     lib.naja_graph_check.argtypes = [vp]

@@ -50,27 +50,33 @@ class Batch:
         check(load().naja_batch_occupancy(len(self.models), self._arr, C.byref(cfg), C.byref(out)))
         return int(out.value)
 
-    def _args(self, X0s, outs, nspc, thinning, nchains, kw):
+    def _args(self, X0s, outs, nspc, thinning, nchains, kw, X_finals=None):
         p, keep = self.models[0].params(nspc, thinning, nchains, **kw)
         X = (C.c_void_p * len(self.models))(*[x.data_ptr() for x in X0s])
         O = (C.c_void_p * len(self.models))(*[o.data_ptr() for o in outs])
-        return p, keep, X, O
+        F = None
+        if X_finals is not None:
+            F = (C.c_void_p * len(self.models))(*[(f.data_ptr() if f is not None else None) for f in X_finals])
+        return p, keep, X, O, F
 
-    def run(self, X0s, outs, nspc, thinning, nchains, shape: Shape = Shape(), seed_stride=1, stream=None, **kw):
-        """X0s[k]: (nchains, d) float64 CUDA tensor; outs[k]: (nspc*nchains, d) CUDA tensor."""
-        p, keep, X, O = self._args(X0s, outs, nspc, thinning, nchains, kw)
+    def run(self, X0s, outs, nspc, thinning, nchains, shape: Shape = Shape(), seed_stride=1, stream=None,
+            X_finals=None, **kw):
+        """X0s[k]: (nchains, d) float64 CUDA tensor; outs[k]: (nspc*nchains, d) CUDA tensor;
+        X_finals[k] (optional): (nchains, d) float64 CUDA tensor receiving model k's last states."""
+        p, keep, X, O, F = self._args(X0s, outs, nspc, thinning, nchains, kw, X_finals)
         cfg = shape.c()
         if stream is None:
             stream = C.c_void_p(torch.cuda.current_stream(outs[0].device).cuda_stream)
-        check(load().naja_chr_run_batched(len(self.models), self._arr, C.byref(p), X, self.d, O, int(seed_stride),
+        check(load().naja_chr_run_batched(len(self.models), self._arr, C.byref(p), X, self.d, O, F, int(seed_stride),
                                           C.byref(cfg), stream))
         del keep
 
-    def capture(self, X0s, outs, nspc, thinning, nchains, shape: Shape = Shape(), seed_stride=1, **kw) -> "Graph":
-        p, keep, X, O = self._args(X0s, outs, nspc, thinning, nchains, kw)
+    def capture(self, X0s, outs, nspc, thinning, nchains, shape: Shape = Shape(), seed_stride=1, X_finals=None,
+                **kw) -> "Graph":
+        p, keep, X, O, F = self._args(X0s, outs, nspc, thinning, nchains, kw, X_finals)
         cfg = shape.c()
         h = C.c_void_p()
-        check(load().naja_chr_capture_batched(len(self.models), self._arr, C.byref(p), X, self.d, O,
+        check(load().naja_chr_capture_batched(len(self.models), self._arr, C.byref(p), X, self.d, O, F,
                                               int(seed_stride), C.byref(cfg), C.byref(h)))
         del keep
         return Graph(h)

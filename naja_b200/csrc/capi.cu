@@ -728,8 +728,8 @@ int batch_sparse_prepare(int nmodels, const naja_polytope* const* models, BatchC
 }
 
 int prep_batch(int nmodels, const naja_polytope* const* models, const naja_chr_params* p, const double* const* X0s,
-               int ldx, void* const* samples, unsigned long long seed_stride, const naja_batch_config* c,
-               BatchPrep* out) {
+               int ldx, void* const* samples, double* const* X_finals, unsigned long long seed_stride,
+               const naja_batch_config* c, BatchPrep* out) {
   if (nmodels <= 0 || !models || !p || !X0s || !samples || !c)
     return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: null or empty argument");
   if (p->nchains <= 0 || p->nspc <= 0 || p->thinning <= 0)
@@ -753,6 +753,8 @@ int prep_batch(int nmodels, const naja_polytope* const* models, const naja_chr_p
     if (P->device != models[0]->device) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: models on different devices");
     if (!X0s[k] || !samples[k] || !is_device_ptr(X0s[k]) || !is_device_ptr(samples[k]))
       return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: X0s and samples must be device pointers");
+    if (X_finals && X_finals[k] && !is_device_ptr(X_finals[k]))
+      return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_run_batched: X_finals must be device pointers");
     lda_max = std::max(lda_max, P->lda);
     m_max = std::max(m_max, P->m);
   }
@@ -761,7 +763,9 @@ int prep_batch(int nmodels, const naja_polytope* const* models, const naja_chr_p
     DeviceGuard g(models[0]->device);
     if (int st = require_local("naja_chr_run_batched", {p->pair_i, p->pair_j, p->pair_c, p->pair_s})) return st;
     for (int k = 0; k < nmodels; ++k)
-      if (int st = require_local("naja_chr_run_batched (X0s[k], samples[k])", {X0s[k], samples[k]})) return st;
+      if (int st = require_local("naja_chr_run_batched (X0s[k], samples[k], X_finals[k])",
+                                 {X0s[k], samples[k], X_finals ? X_finals[k] : nullptr}))
+        return st;
   }
   BatchConfig cfg;
   std::memset(&cfg, 0, sizeof(cfg));
@@ -814,7 +818,7 @@ int prep_batch(int nmodels, const naja_polytope* const* models, const naja_chr_p
     m.X0 = X0s[k];
     m.ldx = ldx;
     m.samples = samples[k];
-    m.X_final = nullptr;
+    m.X_final = X_finals ? X_finals[k] : nullptr;
     m.seed = p->seed + static_cast<unsigned long long>(k) * seed_stride;
     std::memset(&m.sp, 0, sizeof(m.sp));
     if (cfg.sparse) {
@@ -862,10 +866,10 @@ struct GraphHandle {
 }  // namespace
 
 extern "C" int naja_chr_run_batched(int nmodels, const naja_polytope* const* models, const naja_chr_params* p,
-                                    const double* const* X0s, int ldx, void* const* samples,
+                                    const double* const* X0s, int ldx, void* const* samples, double* const* X_finals,
                                     unsigned long long seed_stride, const naja_batch_config* c, void* stream_ptr) {
   BatchPrep b;
-  int st = prep_batch(nmodels, models, p, X0s, ldx, samples, seed_stride, c, &b);
+  int st = prep_batch(nmodels, models, p, X0s, ldx, samples, X_finals, seed_stride, c, &b);
   if (st) return st;
   DeviceGuard g(b.device);
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
@@ -912,11 +916,12 @@ extern "C" int naja_batch_occupancy(int nmodels, const naja_polytope* const* mod
 
 extern "C" int naja_chr_capture_batched(int nmodels, const naja_polytope* const* models, const naja_chr_params* p,
                                         const double* const* X0s, int ldx, void* const* samples,
-                                        unsigned long long seed_stride, const naja_batch_config* c, void** graph) {
+                                        double* const* X_finals, unsigned long long seed_stride,
+                                        const naja_batch_config* c, void** graph) {
   if (!graph) return fail(NAJA_ERR_INVALID_ARGUMENT, "naja_chr_capture_batched: graph is null");
   *graph = nullptr;
   BatchPrep b;
-  int st = prep_batch(nmodels, models, p, X0s, ldx, samples, seed_stride, c, &b);
+  int st = prep_batch(nmodels, models, p, X0s, ldx, samples, X_finals, seed_stride, c, &b);
   if (st) return st;
   DeviceGuard g(b.device);
   GraphHandle* h = new GraphHandle();

@@ -25,13 +25,13 @@
 //     except for the sign of a zero slack, which neither tier's ratio
 //     reads (a zero slack counts as +0) and which no later update can turn
 //     into a different nonzero value.
-//   * Pair steps combine the two columns through a dense scratch column
-//     `ajd` (all zeros between steps): column j is scattered into it, the
-//     pass over column i's entries reads a_j there (0 where column j has no
-//     entry) and marks the shared rows, the pass over column j's entries
-//     skips the marked rows and clears the scratch.  ae = fma(a_i, c_i,
-//     a_j c_j) exactly as the dense kernel forms it.  The combined values
-//     go to a shared array beside the slots; the staged slots are only read.
+//   * Pair steps combine the two staged columns by their row indices, which
+//     are sorted: an entry of column i finds column j's value at its row by
+//     binary search in column j's slot (0 if absent), and an entry of column
+//     j whose row column i also holds is left to that entry.  ae = fma(a_i,
+//     c_i, a_j c_j) exactly as the dense kernel forms it.  The two passes
+//     need no barrier between them and no per-row scratch: the combined
+//     values go to a shared array beside the slots, the slots are only read.
 //   * The FP64 recompute slack = b - A64 x runs over the rows of A64
 //     stored by rows, columns ascending: the dense kernel's fma chain
 //     without its zero terms (padding terms 0 * x_0 change at most the sign
@@ -74,9 +74,9 @@ __device__ __forceinline__ bool sp_is_mark(double v) {
 // Shared memory of one chain: x (FP64), the column offsets, `slots` staged
 // compressed columns of up to max_col entries, the step records and
 // barriers, the cross-warp reduction entries, the abort flag followed by the
-// arrival flags (2 x nw ints), slack and the pair scratch column (m + 1
-// values each), and a pair step's combined values (tail_off: one value per
-// slot entry for column i's entries, then as many for column j's).
+// arrival flags (2 x nw ints), slack (m + 1 values), and a pair step's
+// combined values (tail_off: one value per slot entry for column i's
+// entries, then as many for column j's).
 __host__ __device__ inline Layout make_sparse_layout(int d, int m, int elt, int eb, int max_col, int nw, int slots) {
   Layout L;
   size_t off = 0;
@@ -99,14 +99,26 @@ __host__ __device__ inline Layout make_sparse_layout(int d, int m, int elt, int 
   off = L.flag_off + 16 + 2 * static_cast<size_t>(nw) * 4;
   L.slack_off = align_up(off, 128);
   off = L.slack_off + static_cast<size_t>(m + 1) * elt;
-  L.ajd_off = align_up(off, 16);
-  off = L.ajd_off + static_cast<size_t>(m + 1) * elt;
+  L.ajd_off = 0;
   L.tail_off = align_up(off, 16);
   off = L.tail_off + 2 * (L.slot_bytes / eb) * elt;
   L.total = align_up(off, 128);
   L.slots = slots;
   L.direct = false;
   return L;
+}
+
+// Position of the first entry of a staged column (rows ascending) whose row
+// is >= r, among its n entries.
+template <class E>
+__device__ __forceinline__ int sp_lower_bound(const E* col, int n, int r) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (col[mid].r < r) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
 }
 
 // Barrier over the consumer warps (the producer warp never takes part).
@@ -138,7 +150,6 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.flag_off);
   int* arrived = reinterpret_cast<int*>(smem + L.flag_off + 16);
   Real* slack = reinterpret_cast<Real*>(smem + L.slack_off);
-  Real* ajd = reinterpret_cast<Real*>(smem + L.ajd_off);
   Real* pv = reinterpret_cast<Real*>(smem + L.tail_off);  // combined values, column i's entries
   Real* qv = pv + L.slot_bytes / sizeof(E);                 // ... column j's entries
   const Real* A = T::A(a);
@@ -147,7 +158,6 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
   const int gchain = a.chain_base + chain_local;
 
   for (int j = tid; j < d; j += NT) xs[j] = a.X0[static_cast<size_t>(chain_local) * a.ldx + j];
-  for (int r = tid; r <= m; r += NT) ajd[r] = Real(0);
   consumers_sync<NW>(1);
 
   auto recompute = [&]() {
@@ -282,31 +292,23 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
         reinterpret_cast<const E*>(smem + L.slot_off + static_cast<size_t>(sb < 0 ? 0 : sb) * L.slot_bytes);
     Acc hi = T::acc_hi0(), lo = T::acc_lo0(), lo2 = T::acc_lo20();
     if (kind == kPair) {
-#pragma unroll 4
-      for (int e = tid; e < nb; e += NT) {
-        const E q = eb[e];
-        ajd[q.r] = q.v;
-      }
-      consumers_sync<NW>(3);
-#pragma unroll 4
+      // rows of column i, each with column j's value at that row (0 if none)
       for (int e = tid; e < na; e += NT) {
         const E q = ea[e];
-        const Real w = ajd[q.r];
+        const int pos = sp_lower_bound(eb, nb, q.r);
+        const Real w = (pos < nb && eb[pos].r == q.r) ? eb[pos].v : Real(0);
         const Real ae = T::pair_ae_r(q.v, w, cir, cjr);
-        if (w != Real(0)) ajd[q.r] = sp_mark(Real(0));
         pv[e] = ae;
         T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
       }
-      consumers_sync<NW>(3);
-#pragma unroll 4
+      // rows of column j that column i does not hold; a shared row was taken
+      // with column i's entry, and the marker (-0) makes this entry's update
+      // a no-op below
       for (int e = tid; e < nb; e += NT) {
         const E q = eb[e];
-        const Real w = ajd[q.r];
-        ajd[q.r] = Real(0);
-        // a row shared with column i was taken with that entry: the marker
-        // (-0) makes this entry's update a no-op below
+        const int pos = sp_lower_bound(ea, na, q.r);
         Real ae = sp_mark(Real(0));
-        if (!sp_is_mark(w)) {
+        if (!(pos < na && ea[pos].r == q.r)) {
           ae = T::pair_ae_r(Real(0), q.v, cir, cjr);
           T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
         }
@@ -467,7 +469,7 @@ namespace {
 // model's compressed columns and FP32 tier.  Layout sized for the largest
 // model and the longest column of any model.
 template <int NW>
-__global__ void __launch_bounds__(NW * 32 + 32, NW >= 8 ? 2 : (NW == 4 ? 3 : 4))
+__global__ void __launch_bounds__(NW * 32 + 32, NW >= 8 ? 3 : (NW == 4 ? 4 : 6))
     chr_batched_sparse_kernel(const __grid_constant__ ChrArgs base, const __grid_constant__ Layout L,
                               const ModelDesc* __restrict__ models, const int* __restrict__ item_model,
                               const int* __restrict__ item_chain, int nitems) {

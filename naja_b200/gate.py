@@ -161,3 +161,82 @@ def _violations(torch, A, b, Y):
     for s0 in range(0, Y.shape[0], 50000):
         v += int(((Y[s0:s0 + 50000].double() @ At.T - bt) > tol).sum())
     return v
+
+
+def batch_to_gate(models, roundings, *, nchains=8, thinning=116, chunk_nspc=1000, pair_prob=0.3,
+                  resync_interval=2048, seed=0, budget_s=60.0, rhat_target=1.01, device=0, max_bytes=40 << 30,
+                  shape=None, extra_seconds=0.0):
+    """Many polytopes (models[k] = (A, b)) sampled together in one batched
+    launch per chunk (naja_chr_run_batched, chains continued through
+    X_finals and the step offset), each on its rounding (roundings[k], y = M z
+    + c), until every model's split-R-hat < rhat_target with no bound
+    violations, or the budget.  A model's seconds are the batch's seconds
+    divided by the number of models (plus `extra_seconds`, e.g. the time of
+    computing its rounding).  Returns per-model min-ESS, R-hat, whether it
+    passed, and the aggregate figures."""
+    import torch
+
+    from .batch import Batch, Shape
+
+    dev = torch.device("cuda", device)
+    nm = len(models)
+    d = np.asarray(models[0][0]).shape[1]
+    polys = [Polytope(R.A, R.b, device=device) for R in roundings]
+    dense = any(R.info.get("method") != "identity" for R in roundings)
+    if shape is None:
+        shape = Shape(256, 3, 1, 0, 0) if dense else Shape(256, 8, 1, 0, 1)
+    B = Batch(polys)
+    rows = chunk_nspc * nchains
+    per_chunk = nm * rows * d * 4
+    max_chunks = max(2, int(max_bytes // per_chunk))
+    Ys = [torch.empty((max_chunks * rows, d), dtype=torch.float32, device=dev) for _ in range(nm)]
+    Zs = [torch.empty((rows, d), dtype=torch.float32, device=dev) for _ in range(nm)]
+    X = [torch.from_numpy(np.broadcast_to(R.z0, (nchains, d)).copy()).to(dev) for R in roundings]
+    Xf = [torch.empty_like(x) for x in X]
+    Ms = [torch.from_numpy(np.ascontiguousarray(R.M)).to(dev) for R in roundings]
+    cs = [torch.from_numpy(R.c).to(dev) for R in roundings]
+    passed = np.zeros(nm, dtype=bool)
+    rh_last = np.full(nm, np.inf)
+    dev_ms = 0.0
+    k = 0
+    curve = []
+    while k < max_chunks:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        B.run(X, Zs, chunk_nspc, thinning, nchains, shape=shape, seed_stride=1, X_finals=Xf, seed=seed,
+              pair_prob=pair_prob, resync_interval=resync_interval, step_offset=k * chunk_nspc * thinning)
+        for j in range(nm):
+            backmap(Ms[j], cs[j], Zs[j], mode="fp64", out=Ys[j][k * rows:(k + 1) * rows])
+        k += 1
+        if k >= 2:
+            for j in range(nm):
+                _, rh = ess_rhat(Ys[j][:k * rows], nchains, layout=1, ess=False)
+                rh_last[j] = float(rh.max())
+        e1.record()
+        torch.cuda.synchronize()
+        X, Xf = Xf, X
+        dev_ms += e0.elapsed_time(e1)
+        passed = rh_last < rhat_target
+        curve.append([round(dev_ms / 1e3, 2), round(float(rh_last.max()), 4), int(passed.sum())])
+        if passed.all() or dev_ms / 1e3 >= budget_s:
+            break
+    B.check()
+    spc = k * chunk_nspc
+    stride = -(-spc // ESS_MAX_SERIES)
+    out_models = []
+    for j, (A, b) in enumerate(models):
+        Yk = Ys[j][:k * rows]
+        Ye = Yk.view(spc, nchains, d)[::stride].reshape(-1, d) if stride > 1 else Yk
+        ess, rh = ess_rhat(Ye, nchains, layout=1)
+        viol = _violations(torch, np.asarray(A, dtype=np.float64), np.asarray(b, dtype=np.float64), Yk)
+        out_models.append({"min_ess": float(ess.sum(axis=1).min()), "rhat_max": float(rh_last[j]),
+                           "passed": bool(rh_last[j] < rhat_target and viol == 0), "bounds_violations": int(viol)})
+    for p in polys:
+        p.close()
+    per_model_s = dev_ms / 1e3 / nm + extra_seconds
+    ess_m = np.array([m["min_ess"] for m in out_models])
+    return {"models": nm, "chains_per_model": nchains, "chunks": k, "steps_per_chain": k * chunk_nspc * thinning,
+            "batch_seconds": dev_ms / 1e3, "seconds_per_model": per_model_s,
+            "passed": int(sum(m["passed"] for m in out_models)), "rhat_max": float(rh_last.max()),
+            "min_ess_median": float(np.median(ess_m)), "min_ess_per_s_median": float(np.median(ess_m) / per_model_s),
+            "min_ess_per_s_min": float(ess_m.min() / per_model_s), "curve": curve, "per_model": out_models}

@@ -273,14 +273,27 @@ def features(variant, base):
     return np.log(np.asarray(variant["u_new"], np.float64) / np.asarray(base["u"], np.float64))
 
 
-def factor_targets(samples, rank, torch):
-    """Batched factor_target on the GPU: samples (V, N, dim) -> (V, dim + dim*rank) float64 numpy."""
+def factor_targets(samples, rank, torch, inverse=False):
+    """Batched factor_target on the GPU: samples (V, N, dim) -> (V, dim + dim*rank) float64 numpy.
+
+    inverse=True factors G = Sigma^-1/2 instead of Sigma^1/2, with G's
+    eigenvalues raised to at least their median: the rank-r part then holds
+    the directions in which the samples are thinnest (the ones a rounding
+    must stretch), and no direction is shrunk below the median scale (a
+    short run underestimates the spread of slowly mixing directions, which
+    must not be mistaken for thin ones)."""
     Y = samples.to(torch.float64)
     Y = Y - Y.mean(dim=1, keepdim=True)
     cov = Y.transpose(1, 2) @ Y / (Y.shape[1] - 1)
     w, V = torch.linalg.eigh(cov)
-    w = w.clamp_min(1e-18).flip(-1)
-    V = V.flip(-1)
+    if inverse:
+        g = w.clamp_min(1e-18).rsqrt()
+        g = torch.maximum(g, g.median(dim=-1, keepdim=True).values)
+        w = g * g  # so that s = sqrt(w) = g below
+    w = w.clamp_min(1e-18)
+    order = torch.argsort(w, dim=-1, descending=True)
+    w = torch.gather(w, -1, order)
+    V = torch.gather(V, -1, order[:, None, :].expand_as(V))
     s = w.sqrt()
     floor = s[:, rank:rank + 1] if rank < s.shape[1] else torch.zeros_like(s[:, :1])
     U = V[:, :, :rank] * (s[:, :rank] - floor).clamp_min(0.0).sqrt()[:, None, :]
@@ -292,156 +305,166 @@ def factor_targets(samples, rank, torch):
     return torch.cat([diag.log(), U.reshape(U.shape[0], -1)], dim=1).cpu().numpy()
 
 
-def _sample(polys, Ms, cs, nchains, nspc, thinning, kw, torch, shape=None):
-    """Batched CHR over polytopes given in the rounded space; returns (y samples per model as
-    float32 CUDA tensors, seconds of sampling + map back)."""
+def _rounded_rows(A0M, extra_A, M0, torch):
+    """[A_base M0; extra_A M0] on the device (FP64)."""
+    if extra_A.shape[0] == 0:
+        return A0M
+    E = torch.from_numpy(np.ascontiguousarray(extra_A)).to(A0M.device) @ M0
+    return torch.cat([A0M, E], dim=0)
+
+
+def _targets(base, variants, idx, R0, nchains, nspc, thinning, kw, rank, group, torch, say):
+    """Plain CHR (no per-variant rounding) of each variant in the base
+    model's rounded coordinates w (y = M0 w + c0), batched `group` variants
+    per launch; targets are diag + rank-r factors of the w-sample
+    covariances."""
     from .batch import Batch, Shape
-    from .sampler import backmap
+    from .sampler import Polytope
 
-    d = polys[0].d
     dev = torch.device("cuda")
-    B = Batch(polys)
-    X = [torch.zeros((nchains, d), dtype=torch.float64, device=dev) for _ in polys]
-    outs = [torch.empty((nspc * nchains, d), dtype=torch.float32, device=dev) for _ in polys]
-    ys = [torch.empty_like(o) for o in outs]
-    shape = shape or Shape(512, 3, 1, 0)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    B.run(X, outs, nspc, thinning, nchains, shape=shape, **kw)
-    for k, o in enumerate(outs):
-        if Ms[k] is None:
-            ys[k] = o
-        else:
-            backmap(Ms[k], cs[k], o, mode="fp64", out=ys[k])
-    e1.record()
-    torch.cuda.synchronize()
-    B.check()
-    return ys, e0.elapsed_time(e1) / 1e3
+    M0 = torch.from_numpy(R0.M).to(dev)
+    A0M = torch.from_numpy(base["A"]).to(dev) @ M0
+    d = M0.shape[0]
+    out, t_samp = [], 0.0
+    for g0 in range(0, len(idx), group):
+        ks = idx[g0:g0 + group]
+        polys = []
+        for k in ks:
+            v = variants[k]
+            A = np.vstack([base["A"], v["extra_A"]])
+            b = np.concatenate([base["b"], v["extra_b"]])
+            polys.append(Polytope(_rounded_rows(A0M, v["extra_A"], M0, torch), b - A @ R0.c))
+        B = Batch(polys)
+        X = [torch.zeros((nchains, d), dtype=torch.float64, device=dev) for _ in polys]
+        W = [torch.empty((nspc * nchains, d), dtype=torch.float32, device=dev) for _ in polys]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        B.run(X, W, nspc, thinning, nchains, shape=Shape(256, 3, 1, 0, 0), **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        B.check()
+        t_samp += e0.elapsed_time(e1) / 1e3
+        out.append(factor_targets(torch.stack(W), rank, torch, inverse=True))
+        del W, polys, B
+        say(f"targets: {min(g0 + group, len(idx))}/{len(idx)} variants")
+    return np.concatenate(out), t_samp
 
 
-def _diagnose(ys, nchains):
-    from . import validate as V
+def run_experiment(*, n=2600, d=700, n_train=1024, n_test=16, nchains=8, nspc_train=1500, thinning=116,
+                   pair_prob=0.3, rank=32, hidden=(512, 512), epochs=60, batch=64, lr=1e-3, resync=2048, seed=0,
+                   gate_budget_s=45.0, chunk_nspc=1000, group=256, log=None):
+    """Learned rounding on conditioned variants of the genome-shaped polytope.
 
-    res = []
-    for y in ys:
-        ess, rh = V.ess_rhat(y, nchains, layout=1)
-        res.append((float(V.chain_ess(ess).min()), float(rh.max())))
-    return res
-
-
-def run_experiment(*, n=2600, d=700, n_train=256, n_test=16, nchains=8, nspc_train=500, nspc_test=1000,
-                   thinning=116, pair_prob=0.3, rank=32, hidden=(512, 512), epochs=60, batch=64, lr=1e-3,
-                   resync=2048, seed=0, train_chains=None, log=None):
-    """Plain vs Dikin-rounded vs learned-rounded CHR on held-out conditioned
-    variants of the genome-shaped polytope.  Returns a dict of results."""
+    The base model is rounded once by its whole Dikin ellipsoid, y = M0 w +
+    c0.  A conditioned variant tightens some reactions, which squeezes its
+    polytope along their rows; the network predicts, from the variant's
+    bound ratios, a diagonal-plus-low-rank stretch G = diag(exp(d)) + U U^T
+    in the base coordinates (U: the variant's thinnest directions), and the
+    variant is sampled in z with y = M0 G^-1 z + c0 -- affine, so the uniform
+    target is unchanged.  Targets: factors of the inverse square root of the
+    w-space sample covariances that plain CHR (no per-variant rounding)
+    produces for the training variants (factor_targets, inverse=True).  Held-out variants are then
+    sampled until split-R-hat < 1.01 (batched, one launch per chunk) with:
+    plain CHR, the reference's Dikin preconditioner per variant, the
+    whole-ellipsoid Dikin rounding per variant, the base rounding alone, and
+    the learned rounding; each method's seconds per variant include
+    computing its rounding (network inference for the learned one), and
+    training time is reported separately."""
     import time
 
     import torch
 
-    from . import rounding, synth
-    from .sampler import Polytope
+    from . import gate, rounding, synth
 
     say = log or (lambda *a: None)
     base = synth.genome_shaped(n=n, d=d, density=0.08, seed_T=0, seed_u=1)
     variants = synth.conditioned_variants(base, n_train + n_test, max_reactions=100, seed=seed + 11)
-    A_list = [np.vstack([base["A"], v["extra_A"]]) for v in variants]
-    b_list = [np.concatenate([base["b"], v["extra_b"]]) for v in variants]
     F = np.stack([features(v, base) for v in variants]).astype(np.float32)
     kw = dict(seed=seed, pair_prob=pair_prob, resync_interval=resync)
-
-    # 1. plain CHR on the training variants -> covariance factor targets
     t0 = time.perf_counter()
-    polys = [Polytope(A_list[k], b_list[k]) for k in range(n_train)]
-    ys, t_train_samp = _sample(polys, [None] * n_train, [None] * n_train, train_chains or nchains, nspc_train,
-                               thinning, kw, torch)
-    T = factor_targets(torch.stack(ys), rank, torch)
-    del ys, polys
+    R0 = rounding.dikin_full(base["A"], base["b"], base["start"])
+    t_base = time.perf_counter() - t0
+
+    # 1. targets from plain CHR in the base coordinates
+    t0 = time.perf_counter()
+    T, t_train_samp = _targets(base, variants, list(range(n_train)), R0, nchains, nspc_train, thinning, kw, rank,
+                               group, torch, say)
+    t_targets = time.perf_counter() - t0
     mu, sd = T.mean(axis=0), T.std(axis=0) + 1e-6
     Tn = ((T - mu) / sd).astype(np.float32)
-    # log ratios lie in [log fmin, 0] (most are 0): one global scale, no
-    # per-feature standardisation, which would blow up reactions that are
-    # rarely tightened in the training set
+    # log ratios lie in [log fmin, 0] (most are 0): one global scale
     Fn = (F / 3.0).astype(np.float32)
-    t_targets = time.perf_counter() - t0
-    say(f"targets: {n_train} variants, {t_train_samp:.2f} s sampling, {t_targets:.2f} s total")
 
-    # 2. train on the project's kernels
-    # 90 / 10 split of the training variants; the weights of the epoch with
-    # the lowest validation error are kept (early stopping)
+    # 2. train on the project's kernels; 90 / 10 split, early stopping on validation
     net = RoundingNet((n, *hidden, d + d * rank), seed=seed, lr=lr)
     rng = np.random.default_rng(seed)
     n_val = max(1, n_train // 10)
     fit_idx, val_idx = np.arange(n_train - n_val), np.arange(n_train - n_val, n_train)
     t0 = time.perf_counter()
-    first = None
+    first = loss = None
     best = (float(np.mean(Tn[val_idx] ** 2)), -1, net.snapshot())  # the mean predictor (zero output)
-    curve = []
     for ep in range(epochs):
         perm = rng.permutation(fit_idx)
         for i in range(0, len(perm), batch):
-            idx = perm[i:i + batch]
-            loss = net.train_step(Fn[idx], Tn[idx])
+            loss = net.train_step(Fn[perm[i:i + batch]], Tn[perm[i:i + batch]])
             first = loss if first is None else first
         val = float(np.mean((net.predict(Fn[val_idx]).cpu().numpy() - Tn[val_idx]) ** 2))
-        curve.append(val)
         if val < best[0]:
             best = (val, ep, net.snapshot())
     net.restore(best[2])
     torch.cuda.synchronize()
     t_fit = time.perf_counter() - t0
-    pred_train = net.predict(Fn[fit_idx]).cpu().numpy()
-    train_mse = float(np.mean((pred_train - Tn[fit_idx]) ** 2))
-    say(f"training: {epochs} epochs in {t_fit:.2f} s, loss {first:.4f} -> {loss:.4f}, best validation "
-        f"{best[0]:.4f} at epoch {best[1]}")
+    say(f"training: {epochs} epochs in {t_fit:.2f} s, best validation {best[0]:.4f} at epoch {best[1]}")
 
-    # 3. held-out variants: plain, Dikin, learned
+    # 3. held-out variants
     test = list(range(n_train, n_train + n_test))
-    out = {"train": {"variants": n_train, "epochs": epochs, "seconds": t_fit, "first_loss": first,
-                     "last_loss": loss, "train_mse_std_units": train_mse, "best_epoch": best[1],
-                     "validation_mse_std_units": best[0], "validation_curve": curve,
-                     "target_sampling_seconds": t_train_samp},
-           "test_variants": n_test, "methods": {}}
+    models = [(np.vstack([base["A"], variants[k]["extra_A"]]), np.concatenate([base["b"], variants[k]["extra_b"]]))
+              for k in test]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     pred = net.predict(Fn[test]).cpu().numpy() * sd + mu
-    t_inf = time.perf_counter() - t0
-    # the held-out variants' own covariance factors (for the regression error only)
-    polys = [Polytope(A_list[k], b_list[k]) for k in test]
-    ys, t_plain = _sample(polys, [None] * n_test, [None] * n_test, nchains, nspc_test, thinning, kw, torch)
-    diag_plain = _diagnose(ys, nchains)
-    T_test = factor_targets(torch.stack(ys), rank, torch)
-    out["test_mse_std_units"] = float(np.mean(((pred - T_test) / sd) ** 2))
-    out["test_mse_mean_predictor"] = float(np.mean(((mu - T_test) / sd) ** 2))
-    del ys
-    methods = {"plain": (None, t_plain, diag_plain)}
-    for name in ("dikin", "learned"):
-        Ms, cs, zp = [], [], []
-        t_round = 0.0
-        for j, k in enumerate(test):
+    t_inf = (time.perf_counter() - t0) / n_test
+    T_test, _ = _targets(base, variants, test, R0, nchains, nspc_train, thinning, kw, rank, group, torch, say)
+    out = {"train": {"variants": n_train, "epochs": epochs, "seconds": t_fit, "first_loss": first, "last_loss": loss,
+                     "best_epoch": best[1], "validation_mse_std_units": best[0],
+                     "target_sampling_seconds": t_train_samp, "targets_seconds": t_targets,
+                     "base_rounding_seconds": t_base},
+           "test_variants": n_test,
+           "test_mse_std_units": float(np.mean(((pred - T_test) / sd) ** 2)),
+           "test_mse_mean_predictor": float(np.mean(((mu - T_test) / sd) ** 2)),
+           "methods": {}}
+
+    def compose(A, b, Fm):
+        """Rounding y = M0 Fm z + c0 of (A, b)."""
+        M = R0.M @ Fm
+        return rounding.Rounding(M, R0.c.copy(), A @ M, b - A @ R0.c, np.zeros(d), {"method": "composed"})
+
+    for name in ("plain", "dikin", "dikin_full", "base", "learned"):
+        rs, t_round = [], 0.0
+        for j, (A, b) in enumerate(models):
             t1 = time.perf_counter()
-            if name == "dikin":
-                r = rounding.dikin(A_list[k], b_list[k], np.zeros(d))
+            if name == "plain":
+                r = rounding.identity(A, b, np.zeros(d))
+            elif name == "dikin":
+                r = rounding.dikin(A, b, np.zeros(d))
+            elif name == "dikin_full":
+                r = rounding.dikin_full(A, b, np.zeros(d))
+            elif name == "base":
+                r = compose(A, b, np.eye(d))
             else:
                 logd, U = unpack(pred[j], d, rank)
-                r = rounding.diag_lowrank(logd, U, np.zeros(d), A_list[k], b_list[k])
+                r = compose(A, b, np.linalg.inv(np.diag(np.exp(logd)) + U @ U.T))
             t_round += time.perf_counter() - t1
-            Ms.append(r.M)
-            cs.append(r.c)
-            zp.append(Polytope(r.A, r.b))
-        ys, t_s = _sample(zp, Ms, cs, nchains, nspc_test, thinning, kw, torch)
-        methods[name] = (t_round + (t_inf if name == "learned" else 0.0), t_s, _diagnose(ys, nchains))
-        del ys, zp
-    for name, (t_round, t_s, diag) in methods.items():
-        per = t_s / n_test  # sampling seconds per variant in the batched run
-        ess = np.array([e for e, _ in diag])
-        rh = np.array([r for _, r in diag])
-        out["methods"][name] = {"sampling_seconds": t_s, "rounding_seconds": t_round or 0.0,
-                                "min_ess_per_variant": ess.tolist(), "rhat_max": float(rh.max()),
-                                "rhat_gate_1_01": bool(rh.max() < 1.01),
-                                "min_ess_per_s_median": float(np.median(ess) / per),
-                                "min_ess_per_s_min": float(ess.min() / per)}
+            rs.append(r)
+        extra = t_round / n_test + (t_inf if name == "learned" else 0.0)
+        res = gate.batch_to_gate(models, rs, nchains=nchains, thinning=thinning, chunk_nspc=chunk_nspc,
+                                 pair_prob=pair_prob, resync_interval=resync, seed=seed, budget_s=gate_budget_s,
+                                 extra_seconds=extra)
+        res["rounding_seconds_per_variant"] = extra
+        out["methods"][name] = res
+        say(f"{name}: {res['passed']}/{n_test} passed, median min-ESS/s {res['min_ess_per_s_median']:.2f}")
     m = out["methods"]
-    out["learned_vs_plain"] = m["learned"]["min_ess_per_s_median"] / m["plain"]["min_ess_per_s_median"]
-    out["learned_vs_dikin"] = m["learned"]["min_ess_per_s_median"] / m["dikin"]["min_ess_per_s_median"]
+    for other in ("plain", "dikin", "dikin_full", "base"):
+        out[f"learned_vs_{other}"] = m["learned"]["min_ess_per_s_median"] / max(m[other]["min_ess_per_s_median"],
+                                                                               1e-12)
     return out

@@ -81,3 +81,29 @@ def test_batch_rejects_mixed_dimensions(cuda):
     outs = [torch.empty((20, 5), device=cuda), torch.empty((20, 6), device=cuda)]
     with pytest.raises(InvalidArgument):
         B.run(X, outs, 10, 1, 2)
+
+
+@pytest.mark.parametrize("shape", [Shape(256, 3, 1, 0), Shape(128, 4, 1, 0, sparse=1)], ids=str)
+def test_batched_continuation_with_final_states(cuda, shape):
+    """Two batched launches, the second continuing from the first's X_finals
+    at the step offset where it stopped, give the samples of one launch of
+    twice the length (the chunk spans whole resync periods)."""
+    import torch
+
+    polys, start = _models()
+    P = [Polytope(A, b) for A, b in polys]
+    B = Batch(P)
+    nspc, thin, nch, K = 16, 6, 3, 32  # 96 steps per chunk = 3 resync periods
+    d = len(start)
+    kw = dict(seed=7, seed_stride=3, pair_prob=0.3, resync_interval=K, out_dtype="f64")
+    X = [torch.from_numpy(np.broadcast_to(start, (nch, d)).copy()).cuda() for _ in P]
+    whole = [torch.empty((2 * nspc * nch, d), dtype=torch.float64, device=cuda) for _ in P]
+    B.run(X, whole, 2 * nspc, thin, nch, shape=shape, **kw)
+    Xf = [torch.empty_like(x) for x in X]
+    first = [torch.empty((nspc * nch, d), dtype=torch.float64, device=cuda) for _ in P]
+    second = [torch.empty_like(f) for f in first]
+    B.run(X, first, nspc, thin, nch, shape=shape, X_finals=Xf, **kw)
+    B.run(Xf, second, nspc, thin, nch, shape=shape, step_offset=nspc * thin, **kw)
+    B.check()
+    for k in range(len(P)):
+        assert torch.equal(torch.cat([first[k], second[k]]), whole[k]), k

@@ -166,7 +166,8 @@ def test_affine_hull_reduction(cuda, tmp_path):
     Z = np.load(next((tmp_path / "o1").iterdir()) / "samples.npy")
     assert Z.shape == (600, 11)
     r = _run("sample", "run", "--model-dir", md, "--out-root", tmp_path / "o2", "--n-chains", 2, "--n-samples", 300,
-             "--affine-hull-tol", 1e-9, "--write-npy", "--backmap", "--backmap-mode", "fp64", "--resync-interval", 100)
+             "--affine-hull-tol", 1e-9, "--write-npy", "--backmap", "--backmap-mode", "fp64", "--resync-interval", 100,
+             "--thinning", 50)
     assert r.returncode == 0, r.stderr + r.stdout
     Y = np.load(next((tmp_path / "o2").iterdir()) / "samples.npy").astype(np.float64)
     assert Y.shape == (600, d)
