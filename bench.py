@@ -860,7 +860,7 @@ def main(argv=None):
                     help="learned-rounding section: training variants (0 = skip)")
     ap.add_argument("--learned-test", type=int, default=16)
     ap.add_argument("--learned-nspc", type=int, default=1500, help="samples per chain of each training variant")
-    ap.add_argument("--learned-budget-s", type=float, default=45.0,
+    ap.add_argument("--learned-budget-s", type=float, default=60.0,
                     help="learned-rounding section: seconds per method of the held-out run to the gate")
     ap.add_argument("--learned-epochs", type=int, default=60)
     ap.add_argument("--no-fp64-figure", dest="fp64_figure", action="store_false",

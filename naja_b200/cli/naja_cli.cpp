@@ -568,6 +568,10 @@ int run_sampling(const RunConfig& c) {
         for (int k = 0; k < d; ++k) sx += ar[k] * x0.v[k];
         slack0[r] = b.v[r] - sx;
         double* o = &Ar.v[static_cast<size_t>(r) * dd];
+        // a tight row lies in the span the basis is orthogonal to: its reduced
+        // coefficients are zero (rounding leaves ~1e-16 that, over a zero
+        // slack, would block every chord)
+        if (slack0[r] <= c.affine_hull_tol) continue;
         for (int k = 0; k < d; ++k) {
           const double a = ar[k];
           if (a == 0.0) continue;

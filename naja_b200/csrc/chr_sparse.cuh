@@ -469,7 +469,7 @@ namespace {
 // model's compressed columns and FP32 tier.  Layout sized for the largest
 // model and the longest column of any model.
 template <int NW>
-__global__ void __launch_bounds__(NW * 32 + 32, NW >= 8 ? 3 : (NW == 4 ? 4 : 6))
+__global__ void __launch_bounds__(NW * 32 + 32, NW >= 8 ? 2 : (NW == 4 ? 4 : 6))
     chr_batched_sparse_kernel(const __grid_constant__ ChrArgs base, const __grid_constant__ Layout L,
                               const ModelDesc* __restrict__ models, const int* __restrict__ item_model,
                               const int* __restrict__ item_chain, int nitems) {

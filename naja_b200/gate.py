@@ -184,7 +184,13 @@ def batch_to_gate(models, roundings, *, nchains=8, thinning=116, chunk_nspc=1000
     polys = [Polytope(R.A, R.b, device=device) for R in roundings]
     dense = any(R.info.get("method") != "identity" for R in roundings)
     if shape is None:
-        shape = Shape(256, 3, 1, 0, 0) if dense else Shape(256, 8, 1, 0, 1)
+        # up to one chain per SM: the single-model shape (512 threads, slack in
+        # registers); more chains share SMs with slack in shared memory
+        few = nm * nchains <= _sm_count(torch, dev)
+        if dense:
+            shape = Shape(512, 3, 0, 1, 0) if few else Shape(256, 3, 1, 0, 0)
+        else:
+            shape = Shape(256, 8, 1, 1, 1) if few else Shape(128, 3, 1, 0, 1)
     B = Batch(polys)
     rows = chunk_nspc * nchains
     per_chunk = nm * rows * d * 4
@@ -240,3 +246,7 @@ def batch_to_gate(models, roundings, *, nchains=8, thinning=116, chunk_nspc=1000
             "passed": int(sum(m["passed"] for m in out_models)), "rhat_max": float(rh_last.max()),
             "min_ess_median": float(np.median(ess_m)), "min_ess_per_s_median": float(np.median(ess_m) / per_model_s),
             "min_ess_per_s_min": float(ess_m.min() / per_model_s), "curve": curve, "per_model": out_models}
+
+
+def _sm_count(torch, dev):
+    return torch.cuda.get_device_properties(dev).multi_processor_count
