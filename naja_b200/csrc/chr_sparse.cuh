@@ -26,9 +26,11 @@
 //     reads (a zero slack counts as +0) and which no later update can turn
 //     into a different nonzero value.
 //   * Pair steps combine the two staged columns by their row indices, which
-//     are sorted: an entry of column i finds column j's value at its row by
-//     binary search in column j's slot (0 if absent), and an entry of column
-//     j whose row column i also holds is left to that entry.  ae = fma(a_i,
+//     are sorted: each consumer thread takes a contiguous run of column i's
+//     entries, binary-searches column j's slot once for the run's first row
+//     and merges forward, so every entry finds column j's value at its row
+//     (0 if absent); column j's entries do the same against column i, and one
+//     whose row column i also holds is left to that entry.  ae = fma(a_i,
 //     c_i, a_j c_j) exactly as the dense kernel forms it.  The two passes
 //     need no barrier between them and no per-row scratch: the combined
 //     values go to a shared array beside the slots, the slots are only read.
@@ -292,28 +294,42 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
         reinterpret_cast<const E*>(smem + L.slot_off + static_cast<size_t>(sb < 0 ? 0 : sb) * L.slot_bytes);
     Acc hi = T::acc_hi0(), lo = T::acc_lo0(), lo2 = T::acc_lo20();
     if (kind == kPair) {
-      // rows of column i, each with column j's value at that row (0 if none)
-      for (int e = tid; e < na; e += NT) {
-        const E q = ea[e];
-        const int pos = sp_lower_bound(eb, nb, q.r);
-        const Real w = (pos < nb && eb[pos].r == q.r) ? eb[pos].v : Real(0);
-        const Real ae = T::pair_ae_r(q.v, w, cir, cjr);
-        pv[e] = ae;
-        T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
+      // Each thread takes a contiguous run of a column's entries, finds the
+      // first row of the other column at or after its run by one binary
+      // search and merges forward from there (rows ascend in both columns).
+      // Rows of column i, each with column j's value at that row (0 if none):
+      {
+        const int per = (na + NT - 1) / NT, e0 = tid * per, e1 = min(na, e0 + per);
+        int pos = e0 < e1 ? sp_lower_bound(eb, nb, ea[e0].r) : 0;
+        for (int e = e0; e < e1; ++e) {
+          const E q = ea[e];
+          while (pos < nb && eb[pos].r < q.r) ++pos;
+          const Real w = (pos < nb && eb[pos].r == q.r) ? eb[pos].v : Real(0);
+          const Real ae = T::pair_ae_r(q.v, w, cir, cjr);
+          pv[e] = ae;
+          T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
+        }
       }
       // rows of column j that column i does not hold; a shared row was taken
       // with column i's entry, and the marker (-0) makes this entry's update
       // a no-op below
-      for (int e = tid; e < nb; e += NT) {
-        const E q = eb[e];
-        const int pos = sp_lower_bound(ea, na, q.r);
-        Real ae = sp_mark(Real(0));
-        if (!(pos < na && ea[pos].r == q.r)) {
-          ae = T::pair_ae_r(Real(0), q.v, cir, cjr);
-          T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
+      {
+        const int per = (nb + NT - 1) / NT, e0 = tid * per, e1 = min(nb, e0 + per);
+        int pos = e0 < e1 ? sp_lower_bound(ea, na, eb[e0].r) : 0;
+        for (int e = e0; e < e1; ++e) {
+          const E q = eb[e];
+          while (pos < na && ea[pos].r < q.r) ++pos;
+          Real ae = sp_mark(Real(0));
+          if (!(pos < na && ea[pos].r == q.r)) {
+            ae = T::pair_ae_r(Real(0), q.v, cir, cjr);
+            T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
+          }
+          qv[e] = ae;
         }
-        qv[e] = ae;
       }
+      // the update below reads pv / qv by another thread mapping: with more
+      // than one warp the reduction's barrier orders it, with one warp this
+      if constexpr (NW == 1) __syncwarp();
     } else {
 #pragma unroll 4
       for (int e = tid; e < na; e += NT) {
