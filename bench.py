@@ -146,7 +146,7 @@ class Workload:
                 "thinning": self.thin, "pair_prob": self.pair, "precision": a.precision,
                 "resync_interval": a.resync, "backmap": a.backmap_mode, "rng": "philox", "step_kernel": a.sparse,
                 "rounding": a.rounding,
-                "l2": "256 MiB buffer written between timed steps"}
+                "l2": "256 MiB written between timed steps"}
 
 
 def _gate(torch, W, samples_dev, ess, rhat):
@@ -208,6 +208,83 @@ def _backmap_roofline(W, ms, mode):
     return {"bound": "tensor", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "flops": flops,
             "peak_source": f"{src} bf16" + ("" if mode == "bf16x3" else " / 2 (tf32 rate)"),
             "note": "algorithmic FLOPs 2 n d N; the three split products are not credited"}
+
+
+def _r(x, n=4):
+    """x to n significant digits (numbers only)."""
+    if isinstance(x, float):
+        return float(f"{x:.{n}g}")
+    return x
+
+
+def _compact(line):
+    """The printed line: every section summarised so that the whole line stays
+    near 3,000 characters (the full sections go to --detail-file)."""
+    out = {k: line[k] for k in line if k not in _SECTIONS}
+    rf = dict(line["roofline"])
+    for k in ("bytes_definition", "compressed_bytes_per_chr_step", "chr_steps_per_launch", "kernel_threads"):
+        rf.pop(k, None)
+    if "rounding" in line:
+        out.pop("rounding")
+        out["rounding_s"] = _r(line["rounding"].get("seconds", 0.0), 3)
+    out["roofline"] = {k: _r(v) for k, v in rf.items()}
+    for k in ("value", "ms_per_step", "chr_steps_per_s", "min_ess"):
+        out[k] = _r(line[k], 6)
+    g = line.get("gate")
+    if g:
+        out["gate"] = {k: _r(v) for k, v in g.items() if k in ("rhat_max", "rhat_gate_1_01", "bounds_violations",
+                                                                 "gem_bounds_violations")}
+    bm = line.get("backmap")
+    if bm:
+        out["backmap"] = {"mode": bm["mode"], "ms": _r(bm["ms"]), "max_rel": _r(bm["error_vs_fp64"]["max_rel"], 3),
+                          "tflops": _r(bm["roofline"]["achieved"], 3)}
+    if "e2e" in line:
+        out["e2e"] = {k: _r(v, 5) for k, v in line["e2e"].items() if k != "timing"}
+    if "cpu_baseline" in line:
+        cb = line["cpu_baseline"]
+        out["cpu_baseline"] = {"value": _r(cb["value"]), "unit": cb["unit"], "cores": cb["cores"], "kind": cb["kind"],
+                               "sample": cb["sample"].split(" of the same workload")[0]}
+    if "plain" in line:
+        p = line["plain"]
+        out["plain"] = {"value": _r(p["value"]), "rhat_max": _r(p["rhat_max"]), "M_steps_s": _r(p["chr_steps_per_s"] / 1e6),
+                        "kernel": p["roofline"]["kernel"], "frac": _r(p["roofline"]["frac"], 3)}
+    if "fp64_tier" in line:
+        f = line["fp64_tier"]
+        out["fp64_tier"] = {"value": _r(f["value"]), "ms": _r(f["ms_per_job"]), "rhat_max": _r(f["rhat_max"])}
+    if "unit_cube" in line:
+        u = line["unit_cube"]
+        out["unit_cube"] = {"M_steps_s": _r(u["chr_steps_per_s"] / 1e6), "mean_dev_se": _r(u["mean_max_dev_in_se"], 3),
+                            "var_dev_se": _r(u["var_max_dev_in_se"], 3), "rhat_max": _r(u["rhat_max"])}
+    if "batched" in line:
+        b = line["batched"]
+        sh = b["shape"]
+        out["batched"] = {"M_steps_s": _r(b["chr_steps_per_s"] / 1e6), "frac": _r(b["roofline"]["frac"], 3),
+                          "shape": f"{sh['threads']}t x{sh['slots']} {'columns' if sh['sparse'] else 'dense'}"}
+    if "gate_run" in line:
+        out["gate_run"] = {k: {"reached": r["reached"], "s": _r(r["seconds"], 3), "rhat": _r(r["rhat_max"]),
+                               "min_ess_s": _r(r["min_ess_per_s"]), "viol": r["bounds_violations"]}
+                           for k, r in line["gate_run"]["methods"].items()}
+    if "precision_study" in line:
+        ps = line["precision_study"]
+        out["precision_study"] = {
+            "tier,K,t/fp64,drift_rel,agree_step,viol": [
+                [r["tier"], r["K"], _r(r.get("time_vs_fp64", 1.0), 3), _r(r["slack_drift"]["max_rel"], 2),
+                 r.get("agree_1e-3_through_step_min", 0), r["bound_violations"]] for r in ps["chr"]],
+            "backmap_ms_maxrel": {m: [_r(v["ms_200k"], 3), _r(v["max_rel"], 2)] for m, v in ps["backmap"].items()}}
+    if "learned_rounding" in line:
+        lr = line["learned_rounding"]
+        out["learned_rounding"] = {
+            "train": lr["train"]["variants"], "test": lr["test_variants"],
+            "mse": [_r(lr["test_mse_std_units"]), _r(lr["test_mse_mean_predictor"])],
+            "min_ess_s": {k: _r(v["min_ess_per_s_median"]) for k, v in lr["methods"].items()},
+            "rhat": {k: _r(v["rhat_max"]) for k, v in lr["methods"].items()},
+            "passed": {k: v["passed"] for k, v in lr["methods"].items()},
+            **{k: _r(v, 3) for k, v in lr.items() if k.startswith("learned_vs_")}}
+    return out
+
+
+_SECTIONS = ("roofline", "gate", "backmap", "e2e", "cpu_baseline", "plain", "fp64_tier", "unit_cube", "batched",
+             "gate_run", "precision_study", "learned_rounding", "reference_semantics_validate", "job_ms", "chr_ms")
 
 
 def _stats(v):
@@ -385,11 +462,12 @@ def _ours(a, rank, world):
         line["precision_study"] = _precision_study(a)
     if rank == 0 and a.learned_train > 0:
         line["learned_rounding"], detail["learned_rounding"] = _learned(a)
+    detail["line"] = line
     if rank == 0 and a.detail_file:
         Path(a.detail_file).parent.mkdir(parents=True, exist_ok=True)
         Path(a.detail_file).write_text(json.dumps(detail))
     P.close()
-    return line
+    return _compact(line)
 
 
 def _e2e(a, W, torch, dev, min_ess):

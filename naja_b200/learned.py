@@ -352,7 +352,7 @@ def _targets(base, variants, idx, R0, nchains, nspc, thinning, kw, rank, group, 
 
 def run_experiment(*, n=2600, d=700, n_train=1024, n_test=16, nchains=8, nspc_train=1500, thinning=116,
                    pair_prob=0.3, rank=32, hidden=(512, 512), epochs=60, batch=64, lr=1e-3, resync=2048, seed=0,
-                   gate_budget_s=45.0, chunk_nspc=1000, group=256, log=None):
+                   gate_budget_s=45.0, chunk_nspc=4000, group=256, log=None):
     """Learned rounding on conditioned variants of the genome-shaped polytope.
 
     The base model is rounded once by its whole Dikin ellipsoid, y = M0 w +
