@@ -56,6 +56,7 @@ struct ChrLaunchConfig {
   int cluster;    // CTAs per chain (thread-block cluster); 1 = one CTA per chain
   int slice_lda;  // rows a CTA's column slot holds (cluster > 1), padded to 32
   int max_col;    // sparse-column kernel: entries of the longest compressed column
+  int pair_scatter;  // sparse-column kernel: 1 = pair steps through a scratch column, 0 = by search
 };
 
 // Compressed columns of A for the sparse-column kernel, in the tier's

@@ -88,6 +88,7 @@ int plan_single(int precision, int m, int d, int lda, int tpb, int max_slots, Ch
   out->cluster = 1;
   out->slice_lda = lda;
   out->max_col = 0;
+  out->pair_scatter = 0;
   return NAJA_OK;
 }
 
@@ -128,6 +129,7 @@ int plan_cluster(int precision, int m, int d, int tpb, int max_slots, int cs, Ch
   out->cluster = cs;
   out->slice_lda = slda;
   out->max_col = 0;
+  out->pair_scatter = 0;
   return NAJA_OK;
 }
 }  // namespace

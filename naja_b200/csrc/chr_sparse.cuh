@@ -25,15 +25,22 @@
 //     except for the sign of a zero slack, which neither tier's ratio
 //     reads (a zero slack counts as +0) and which no later update can turn
 //     into a different nonzero value.
-//   * Pair steps combine the two staged columns by their row indices, which
-//     are sorted: each consumer thread takes a contiguous run of column i's
-//     entries, binary-searches column j's slot once for the run's first row
-//     and merges forward, so every entry finds column j's value at its row
-//     (0 if absent); column j's entries do the same against column i, and one
-//     whose row column i also holds is left to that entry.  ae = fma(a_i,
-//     c_i, a_j c_j) exactly as the dense kernel forms it.  The two passes
-//     need no barrier between them and no per-row scratch: the combined
-//     values go to a shared array beside the slots, the slots are only read.
+//   * Pair steps combine the two columns in one of two ways (template SCAT,
+//     same values either way):
+//       scatter (single-model kernel, when it fits): column j is scattered
+//         into a dense scratch column `ajd` (all zeros between steps), the
+//         pass over column i's entries reads a_j there (0 where column j has
+//         no entry) and marks the shared rows, the pass over column j's
+//         entries skips the marked rows and clears the scratch -- two more
+//         barriers per pair step and m values of shared memory;
+//       search (batched kernel, or when the scratch column does not fit):
+//         an entry of column i finds column j's value at its row by binary
+//         search in column j's slot (rows ascend), and an entry of column j
+//         whose row column i also holds is left to that entry -- no scratch
+//         and no extra barrier, so more chains fit on an SM.
+//     ae = fma(a_i, c_i, a_j c_j) exactly as the dense kernel forms it.  The
+//     combined values go to a shared array beside the slots; the staged
+//     slots are only read.
 //   * The FP64 recompute slack = b - A64 x runs over the rows of A64
 //     stored by rows, columns ascending: the dense kernel's fma chain
 //     without its zero terms (padding terms 0 * x_0 change at most the sign
@@ -76,10 +83,12 @@ __device__ __forceinline__ bool sp_is_mark(double v) {
 // Shared memory of one chain: x (FP64), the column offsets, `slots` staged
 // compressed columns of up to max_col entries, the step records and
 // barriers, the cross-warp reduction entries, the abort flag followed by the
-// arrival flags (2 x nw ints), slack (m + 1 values), and a pair step's
-// combined values (tail_off: one value per slot entry for column i's
-// entries, then as many for column j's).
-__host__ __device__ inline Layout make_sparse_layout(int d, int m, int elt, int eb, int max_col, int nw, int slots) {
+// arrival flags (2 x nw ints), slack (m + 1 values), with `scatter` the
+// pair scratch column (m + 1 values), and a pair step's combined values
+// (tail_off: one value per slot entry for column i's entries, then as many
+// for column j's).
+__host__ __device__ inline Layout make_sparse_layout(int d, int m, int elt, int eb, int max_col, int nw, int slots,
+                                                     bool scatter = false) {
   Layout L;
   size_t off = 0;
   L.x_off = 0;
@@ -102,6 +111,10 @@ __host__ __device__ inline Layout make_sparse_layout(int d, int m, int elt, int 
   L.slack_off = align_up(off, 128);
   off = L.slack_off + static_cast<size_t>(m + 1) * elt;
   L.ajd_off = 0;
+  if (scatter) {
+    L.ajd_off = align_up(off, 16);
+    off = L.ajd_off + static_cast<size_t>(m + 1) * elt;
+  }
   L.tail_off = align_up(off, 16);
   off = L.tail_off + 2 * (L.slot_bytes / eb) * elt;
   L.total = align_up(off, 128);
@@ -134,7 +147,7 @@ __device__ __forceinline__ void consumers_sync(uint32_t id) {
 }
 
 // The consumer warps of one chain.
-template <class Real, int NW>
+template <class Real, int NW, bool SCAT>
 __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const Layout& L, unsigned char* smem,
                                      int chain_local) {
   using T = Tier<Real>;
@@ -152,6 +165,7 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.flag_off);
   int* arrived = reinterpret_cast<int*>(smem + L.flag_off + 16);
   Real* slack = reinterpret_cast<Real*>(smem + L.slack_off);
+  Real* ajd = reinterpret_cast<Real*>(smem + L.ajd_off);  // SCAT only
   Real* pv = reinterpret_cast<Real*>(smem + L.tail_off);  // combined values, column i's entries
   Real* qv = pv + L.slot_bytes / sizeof(E);                 // ... column j's entries
   const Real* A = T::A(a);
@@ -160,6 +174,9 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
   const int gchain = a.chain_base + chain_local;
 
   for (int j = tid; j < d; j += NT) xs[j] = a.X0[static_cast<size_t>(chain_local) * a.ldx + j];
+  if constexpr (SCAT) {
+    for (int r = tid; r <= m; r += NT) ajd[r] = Real(0);
+  }
   consumers_sync<NW>(1);
 
   auto recompute = [&]() {
@@ -293,43 +310,60 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
     const E* eb =
         reinterpret_cast<const E*>(smem + L.slot_off + static_cast<size_t>(sb < 0 ? 0 : sb) * L.slot_bytes);
     Acc hi = T::acc_hi0(), lo = T::acc_lo0(), lo2 = T::acc_lo20();
-    if (kind == kPair) {
-      // Each thread takes a contiguous run of a column's entries, finds the
-      // first row of the other column at or after its run by one binary
-      // search and merges forward from there (rows ascend in both columns).
-      // Rows of column i, each with column j's value at that row (0 if none):
-      {
-        const int per = (na + NT - 1) / NT, e0 = tid * per, e1 = min(na, e0 + per);
-        int pos = e0 < e1 ? sp_lower_bound(eb, nb, ea[e0].r) : 0;
-        for (int e = e0; e < e1; ++e) {
-          const E q = ea[e];
-          while (pos < nb && eb[pos].r < q.r) ++pos;
-          const Real w = (pos < nb && eb[pos].r == q.r) ? eb[pos].v : Real(0);
-          const Real ae = T::pair_ae_r(q.v, w, cir, cjr);
-          pv[e] = ae;
+    if (kind == kPair && SCAT) {
+#pragma unroll 4
+      for (int e = tid; e < nb; e += NT) {
+        const E q = eb[e];
+        ajd[q.r] = q.v;
+      }
+      consumers_sync<NW>(3);
+#pragma unroll 4
+      for (int e = tid; e < na; e += NT) {
+        const E q = ea[e];
+        const Real w = ajd[q.r];
+        const Real ae = T::pair_ae_r(q.v, w, cir, cjr);
+        if (w != Real(0)) ajd[q.r] = sp_mark(Real(0));
+        pv[e] = ae;
+        T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
+      }
+      consumers_sync<NW>(3);
+#pragma unroll 4
+      for (int e = tid; e < nb; e += NT) {
+        const E q = eb[e];
+        const Real w = ajd[q.r];
+        ajd[q.r] = Real(0);
+        // a row shared with column i was taken with that entry: the marker
+        // (-0) makes this entry's update a no-op below
+        Real ae = sp_mark(Real(0));
+        if (!sp_is_mark(w)) {
+          ae = T::pair_ae_r(Real(0), q.v, cir, cjr);
           T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
         }
+        qv[e] = ae;
+      }
+    } else if (kind == kPair) {
+      // rows of column i, each with column j's value at that row (0 if none)
+      for (int e = tid; e < na; e += NT) {
+        const E q = ea[e];
+        const int pos = sp_lower_bound(eb, nb, q.r);
+        const Real w = (pos < nb && eb[pos].r == q.r) ? eb[pos].v : Real(0);
+        const Real ae = T::pair_ae_r(q.v, w, cir, cjr);
+        pv[e] = ae;
+        T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
       }
       // rows of column j that column i does not hold; a shared row was taken
       // with column i's entry, and the marker (-0) makes this entry's update
       // a no-op below
-      {
-        const int per = (nb + NT - 1) / NT, e0 = tid * per, e1 = min(nb, e0 + per);
-        int pos = e0 < e1 ? sp_lower_bound(ea, na, eb[e0].r) : 0;
-        for (int e = e0; e < e1; ++e) {
-          const E q = eb[e];
-          while (pos < na && ea[pos].r < q.r) ++pos;
-          Real ae = sp_mark(Real(0));
-          if (!(pos < na && ea[pos].r == q.r)) {
-            ae = T::pair_ae_r(Real(0), q.v, cir, cjr);
-            T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
-          }
-          qv[e] = ae;
+      for (int e = tid; e < nb; e += NT) {
+        const E q = eb[e];
+        const int pos = sp_lower_bound(ea, na, q.r);
+        Real ae = sp_mark(Real(0));
+        if (!(pos < na && ea[pos].r == q.r)) {
+          ae = T::pair_ae_r(Real(0), q.v, cir, cjr);
+          T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
         }
+        qv[e] = ae;
       }
-      // the update below reads pv / qv by another thread mapping: with more
-      // than one warp the reduction's barrier orders it, with one warp this
-      if constexpr (NW == 1) __syncwarp();
     } else {
 #pragma unroll 4
       for (int e = tid; e < na; e += NT) {
@@ -420,7 +454,7 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
   }
 }
 
-template <class Real, int NW>
+template <class Real, int NW, bool SCAT>
 __global__ void __launch_bounds__(NW * 32 + 32, 1)
     chr_sparse_kernel(const __grid_constant__ ChrArgs a, const __grid_constant__ SpArgs sp,
                       const __grid_constant__ Layout L) {
@@ -444,15 +478,16 @@ __global__ void __launch_bounds__(NW * 32 + 32, 1)
       producer_entry<Real, true>(a, L, smem, blockIdx.x, &sp, cs, static_cast<int>(sizeof(SpEntry<Real>)));
     return;
   }
-  run_sparse_consumers<Real, NW>(a, sp, L, smem, blockIdx.x);
+  run_sparse_consumers<Real, NW, SCAT>(a, sp, L, smem, blockIdx.x);
 }
 
-template <class Real, int NW>
+template <class Real, int NW, bool SCAT>
 int launch_sparse(const ChrArgs& a, const SpArgs& sp, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream) {
-  auto kern = chr_sparse_kernel<Real, NW>;
+  auto kern = chr_sparse_kernel<Real, NW, SCAT>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(cfg.smem));
   if (e != cudaSuccess) return NAJA_ERR_CUDA;
-  const Layout L = make_sparse_layout(a.d, a.m, sizeof(Real), sizeof(SpEntry<Real>), cfg.max_col, NW, cfg.slots);
+  const Layout L =
+      make_sparse_layout(a.d, a.m, sizeof(Real), sizeof(SpEntry<Real>), cfg.max_col, NW, cfg.slots, SCAT);
   kern<<<nchains, NW * 32 + 32, cfg.smem, stream>>>(a, sp, L);
   return cudaGetLastError() == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
 }
@@ -460,12 +495,18 @@ int launch_sparse(const ChrArgs& a, const SpArgs& sp, int nchains, const ChrLaun
 template <class Real>
 int launch_sparse_nw(const ChrArgs& a, const SpArgs& sp, int nchains, const ChrLaunchConfig& cfg,
                      cudaStream_t stream) {
+  const bool sc = cfg.pair_scatter != 0;
   switch (cfg.threads) {
-    case 32: return launch_sparse<Real, 1>(a, sp, nchains, cfg, stream);
-    case 64: return launch_sparse<Real, 2>(a, sp, nchains, cfg, stream);
-    case 128: return launch_sparse<Real, 4>(a, sp, nchains, cfg, stream);
-    case 256: return launch_sparse<Real, 8>(a, sp, nchains, cfg, stream);
-    case 512: return launch_sparse<Real, 16>(a, sp, nchains, cfg, stream);
+    case 32: return sc ? launch_sparse<Real, 1, true>(a, sp, nchains, cfg, stream)
+                       : launch_sparse<Real, 1, false>(a, sp, nchains, cfg, stream);
+    case 64: return sc ? launch_sparse<Real, 2, true>(a, sp, nchains, cfg, stream)
+                       : launch_sparse<Real, 2, false>(a, sp, nchains, cfg, stream);
+    case 128: return sc ? launch_sparse<Real, 4, true>(a, sp, nchains, cfg, stream)
+                        : launch_sparse<Real, 4, false>(a, sp, nchains, cfg, stream);
+    case 256: return sc ? launch_sparse<Real, 8, true>(a, sp, nchains, cfg, stream)
+                        : launch_sparse<Real, 8, false>(a, sp, nchains, cfg, stream);
+    case 512: return sc ? launch_sparse<Real, 16, true>(a, sp, nchains, cfg, stream)
+                        : launch_sparse<Real, 16, false>(a, sp, nchains, cfg, stream);
     default: return NAJA_ERR_UNSUPPORTED;
   }
 }
@@ -534,7 +575,7 @@ __global__ void __launch_bounds__(NW * 32 + 32, NW >= 8 ? 2 : (NW == 4 ? 4 : 6))
       if (threadIdx.x == NT)
         producer_entry<Real, true>(item_args, L, smem, ch, &item_sp, cs, static_cast<int>(sizeof(SpEntry<Real>)));
     } else {
-      run_sparse_consumers<Real, NW>(item_args, item_sp, L, smem, ch);
+      run_sparse_consumers<Real, NW, false>(item_args, item_sp, L, smem, ch);
     }
     __syncthreads();
     if (threadIdx.x == 0) {

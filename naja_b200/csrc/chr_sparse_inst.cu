@@ -22,14 +22,25 @@ int chr_sparse_plan(int precision, int m, int d, int max_col, double mean_col, i
   const bool f64 = precision == NAJA_PREC_FP64;
   const int elt = f64 ? 8 : 4, eb = f64 ? kSpEntryBytes64 : kSpEntryBytes32;
   const int nw = threads / 32;
-  int slots = kMaxSlots;
-  if (max_slots > 0 && max_slots < slots) slots = max_slots;
-  Layout L = make_sparse_layout(d, m, elt, eb, max_col, nw, slots);
-  while (slots > 3 && L.total > kSmemBudget) {
-    --slots;
-    L = make_sparse_layout(d, m, elt, eb, max_col, nw, slots);
+  // Pair steps through a scratch column where it fits (fewer instructions per
+  // step); otherwise by search (no scratch column, m values less).
+  int slots = 0;
+  bool scatter = true;
+  Layout L;
+  for (int sc = 1; sc >= 0 && slots == 0; --sc) {
+    int s = kMaxSlots;
+    if (max_slots > 0 && max_slots < s) s = max_slots;
+    L = make_sparse_layout(d, m, elt, eb, max_col, nw, s, sc != 0);
+    while (s > 3 && L.total > kSmemBudget) {
+      --s;
+      L = make_sparse_layout(d, m, elt, eb, max_col, nw, s, sc != 0);
+    }
+    if (s >= 3 && L.total <= kSmemBudget) {
+      slots = s;
+      scatter = sc != 0;
+    }
   }
-  if (slots < 3 || L.total > kSmemBudget) return NAJA_ERR_UNSUPPORTED;
+  if (slots == 0) return NAJA_ERR_UNSUPPORTED;
   out->threads = threads;
   out->rows = 0;
   out->slots = slots;
@@ -37,6 +48,7 @@ int chr_sparse_plan(int precision, int m, int d, int max_col, double mean_col, i
   out->cluster = 1;
   out->slice_lda = 0;
   out->max_col = max_col;
+  out->pair_scatter = scatter ? 1 : 0;
   return NAJA_OK;
 }
 

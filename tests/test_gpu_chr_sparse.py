@@ -185,3 +185,24 @@ def test_automatic_choice(cuda):
     ch = P.kernel_choice(10, 1, 4, sparse="columns")
     assert ch["threads"] == 64 and ch["slots"] >= 3 and ch["smem"] > 0
     assert P.kernel_choice(10, 1, 4, sparse="columns", tpb=256)["threads"] == 256
+
+
+@pytest.mark.parametrize("pair_mode", [1, 2])
+def test_columns_pair_steps_by_search_when_scratch_does_not_fit(cuda, pair_mode):
+    """m = 12,000 rows in the FP64 tier: slack and a scratch column of 12,001
+    doubles each leave no room for three staged columns, so pair steps
+    combine the columns by binary search; the samples stay the oracle's."""
+    A, b, x0 = _genome(6000, 100, 21)
+    assert A.shape[0] == 12000
+    P = Polytope(A, b)
+    assert P.kernel_choice(10, 5, 3, precision="fp64", pair_prob=0.5)["kernel"] == "columns"
+    d = A.shape[1]
+    rng = np.random.default_rng(2)
+    perm = rng.permutation(d)
+    th = rng.uniform(-np.pi, np.pi, d // 2)
+    pairs = (perm[0::2], perm[1::2], np.cos(th), np.sin(th)) if pair_mode == 2 else None
+    kw = dict(seed=9, pair_prob=0.5, precision="fp64", pair_mode=pair_mode, pairs=pairs)
+    got = P.run(x0, 30, 5, 3, out_dtype="f64", sparse="columns", **kw)
+    P.check()
+    ref = _oracle(A, b, x0, 30, 5, 3, **kw)
+    assert np.array_equal(got, ref), np.abs(got - ref).max()
