@@ -33,11 +33,14 @@
 //         no entry) and marks the shared rows, the pass over column j's
 //         entries skips the marked rows and clears the scratch -- two more
 //         barriers per pair step and m values of shared memory;
-//       search (batched kernel, or when the scratch column does not fit):
-//         an entry of column i finds column j's value at its row by binary
-//         search in column j's slot (rows ascend), and an entry of column j
-//         whose row column i also holds is left to that entry -- no scratch
-//         and no extra barrier, so more chains fit on an SM.
+//       bitmap (batched kernel, or when the scratch column does not fit):
+//         both columns' rows are set in two bitmaps of m + 1 bits (atomicOr,
+//         one barrier); an entry of column i whose row column j also holds
+//         (its bit set) finds column j's value there by binary search in
+//         column j's slot (rows ascend), and an entry of column j whose row
+//         column i holds is left to that entry; the update pass clears the
+//         bits.  2 (m + 1) bits instead of m + 1 values of shared memory, so
+//         more chains fit on an SM, and only the few shared rows search.
 //     ae = fma(a_i, c_i, a_j c_j) exactly as the dense kernel forms it.  The
 //     combined values go to a shared array beside the slots; the staged
 //     slots are only read.
@@ -80,6 +83,9 @@ __device__ __forceinline__ bool sp_is_mark(double v) {
   return static_cast<unsigned long long>(__double_as_longlong(v)) == 0x8000000000000000ull;
 }
 
+// 32-bit words of one row bitmap (rows 0..m, row m the padding row).
+__host__ __device__ inline size_t sp_bitmap_words(int m) { return (static_cast<size_t>(m) + 32) / 32; }
+
 // Shared memory of one chain: x (FP64), the column offsets, `slots` staged
 // compressed columns of up to max_col entries, the step records and
 // barriers, the cross-warp reduction entries, the abort flag followed by the
@@ -110,11 +116,9 @@ __host__ __device__ inline Layout make_sparse_layout(int d, int m, int elt, int 
   off = L.flag_off + 16 + 2 * static_cast<size_t>(nw) * 4;
   L.slack_off = align_up(off, 128);
   off = L.slack_off + static_cast<size_t>(m + 1) * elt;
-  L.ajd_off = 0;
-  if (scatter) {
-    L.ajd_off = align_up(off, 16);
-    off = L.ajd_off + static_cast<size_t>(m + 1) * elt;
-  }
+  // the pair scratch column, or the two row bitmaps
+  L.ajd_off = align_up(off, 16);
+  off = L.ajd_off + (scatter ? static_cast<size_t>(m + 1) * elt : 2 * sp_bitmap_words(m) * sizeof(uint32_t));
   L.tail_off = align_up(off, 16);
   off = L.tail_off + 2 * (L.slot_bytes / eb) * elt;
   L.total = align_up(off, 128);
@@ -165,7 +169,10 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + L.flag_off);
   int* arrived = reinterpret_cast<int*>(smem + L.flag_off + 16);
   Real* slack = reinterpret_cast<Real*>(smem + L.slack_off);
-  Real* ajd = reinterpret_cast<Real*>(smem + L.ajd_off);  // SCAT only
+  Real* ajd = reinterpret_cast<Real*>(smem + L.ajd_off);           // SCAT
+  uint32_t* bits_j = reinterpret_cast<uint32_t*>(smem + L.ajd_off);  // !SCAT: rows of column j,
+  const int nwords = static_cast<int>(sp_bitmap_words(a.m));
+  uint32_t* bits_i = bits_j + nwords;                                 // then rows of column i
   Real* pv = reinterpret_cast<Real*>(smem + L.tail_off);  // combined values, column i's entries
   Real* qv = pv + L.slot_bytes / sizeof(E);                 // ... column j's entries
   const Real* A = T::A(a);
@@ -176,6 +183,8 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
   for (int j = tid; j < d; j += NT) xs[j] = a.X0[static_cast<size_t>(chain_local) * a.ldx + j];
   if constexpr (SCAT) {
     for (int r = tid; r <= m; r += NT) ajd[r] = Real(0);
+  } else {
+    for (int w = tid; w < 2 * nwords; w += NT) bits_j[w] = 0u;
   }
   consumers_sync<NW>(1);
 
@@ -342,11 +351,20 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
         qv[e] = ae;
       }
     } else if (kind == kPair) {
+      for (int e = tid; e < nb; e += NT) {
+        const int r = eb[e].r;
+        atomicOr(&bits_j[r >> 5], 1u << (r & 31));
+      }
+      for (int e = tid; e < na; e += NT) {
+        const int r = ea[e].r;
+        atomicOr(&bits_i[r >> 5], 1u << (r & 31));
+      }
+      consumers_sync<NW>(3);
       // rows of column i, each with column j's value at that row (0 if none)
       for (int e = tid; e < na; e += NT) {
         const E q = ea[e];
-        const int pos = sp_lower_bound(eb, nb, q.r);
-        const Real w = (pos < nb && eb[pos].r == q.r) ? eb[pos].v : Real(0);
+        Real w = Real(0);
+        if ((bits_j[q.r >> 5] >> (q.r & 31)) & 1u) w = eb[sp_lower_bound(eb, nb, q.r)].v;
         const Real ae = T::pair_ae_r(q.v, w, cir, cjr);
         pv[e] = ae;
         T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
@@ -356,14 +374,16 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
       // a no-op below
       for (int e = tid; e < nb; e += NT) {
         const E q = eb[e];
-        const int pos = sp_lower_bound(ea, na, q.r);
         Real ae = sp_mark(Real(0));
-        if (!(pos < na && ea[pos].r == q.r)) {
+        if (!((bits_i[q.r >> 5] >> (q.r & 31)) & 1u)) {
           ae = T::pair_ae_r(Real(0), q.v, cir, cjr);
           T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
         }
         qv[e] = ae;
       }
+      // the update pass clears bits other threads tested: with more than one
+      // warp the reduction's barrier orders the two, with one warp this
+      if constexpr (NW == 1) __syncwarp();
     } else {
 #pragma unroll 4
       for (int e = tid; e < na; e += NT) {
@@ -414,18 +434,20 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
     // combined value of -0, whose update would only change the sign of a
     // zero slack) is skipped.
     if (kind == kPair) {
+      // (bitmap variant: every bit the step set is cleared here, after the
+      // reduction's barrier, so the next pair step starts from zeros)
 #pragma unroll 4
       for (int e = tid; e < na; e += NT) {
         const int r = ea[e].r;
         slack[r] = T::slack_update(slack[r], alpha, pv[e]);
+        if constexpr (!SCAT) atomicAnd(&bits_i[r >> 5], ~(1u << (r & 31)));
       }
 #pragma unroll 4
       for (int e = tid; e < nb; e += NT) {
         const Real ae = qv[e];
-        if (!sp_is_mark(ae)) {
-          const int r = eb[e].r;
-          slack[r] = T::slack_update(slack[r], alpha, ae);
-        }
+        const int r = eb[e].r;
+        if (!sp_is_mark(ae)) slack[r] = T::slack_update(slack[r], alpha, ae);
+        if constexpr (!SCAT) atomicAnd(&bits_j[r >> 5], ~(1u << (r & 31)));
       }
     } else {
 #pragma unroll 4
