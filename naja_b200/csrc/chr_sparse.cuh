@@ -140,6 +140,9 @@ __device__ __forceinline__ int sp_lower_bound(const E* col, int n, int r) {
   return lo;
 }
 
+// Entries a consumer thread loads together in a coordinate step's passes.
+constexpr int kSpBatch = 4;
+
 // Barrier over the consumer warps (the producer warp never takes part).
 template <int NW>
 __device__ __forceinline__ void consumers_sync(uint32_t id) {
@@ -385,10 +388,22 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
       // warp the reduction's barrier orders the two, with one warp this
       if constexpr (NW == 1) __syncwarp();
     } else {
-#pragma unroll 4
-      for (int e = tid; e < na; e += NT) {
-        const E q = ea[e];
-        T::acc(hi, lo, lo2, T::ratio(q.v, slack[q.r]));
+      // kSpBatch entries per thread at a time: their loads are all issued
+      // before the first ratio needs one (the per-entry chain is load, load,
+      // divide)
+      for (int e0 = tid; e0 < na; e0 += kSpBatch * NT) {
+        E q[kSpBatch];
+        Real sv[kSpBatch];
+#pragma unroll
+        for (int u = 0; u < kSpBatch; ++u) {
+          const int e = e0 + u * NT;
+          q[u] = e < na ? ea[e] : E{Real(0), m};
+        }
+#pragma unroll
+        for (int u = 0; u < kSpBatch; ++u) sv[u] = slack[q[u].r];
+#pragma unroll
+        for (int u = 0; u < kSpBatch; ++u)
+          if (e0 + u * NT < na) T::acc(hi, lo, lo2, T::ratio(q[u].v, sv[u]));
       }
     }
     reduce(hi, lo, lo2);
@@ -450,10 +465,20 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
         if constexpr (!SCAT) atomicAnd(&bits_j[r >> 5], ~(1u << (r & 31)));
       }
     } else {
-#pragma unroll 4
-      for (int e = tid; e < na; e += NT) {
-        const E q = ea[e];
-        slack[q.r] = T::slack_update(slack[q.r], alpha, q.v);
+      for (int e0 = tid; e0 < na; e0 += kSpBatch * NT) {
+        E q[kSpBatch];
+        Real sv[kSpBatch];
+#pragma unroll
+        for (int u = 0; u < kSpBatch; ++u) {
+          const int e = e0 + u * NT;
+          q[u] = e < na ? ea[e] : E{Real(0), m};
+        }
+#pragma unroll
+        for (int u = 0; u < kSpBatch; ++u) sv[u] = slack[q[u].r];
+        // entries past na stand for the scratch row m and are not written
+#pragma unroll
+        for (int u = 0; u < kSpBatch; ++u)
+          if (e0 + u * NT < na) slack[q[u].r] = T::slack_update(sv[u], alpha, q[u].v);
       }
     }
     __syncwarp();
