@@ -363,26 +363,57 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
         atomicOr(&bits_i[r >> 5], 1u << (r & 31));
       }
       consumers_sync<NW>(3);
-      // rows of column i, each with column j's value at that row (0 if none)
-      for (int e = tid; e < na; e += NT) {
-        const E q = ea[e];
-        Real w = Real(0);
-        if ((bits_j[q.r >> 5] >> (q.r & 31)) & 1u) w = eb[sp_lower_bound(eb, nb, q.r)].v;
-        const Real ae = T::pair_ae_r(q.v, w, cir, cjr);
-        pv[e] = ae;
-        T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
+      // rows of column i, each with column j's value at that row (0 if none);
+      // kSpBatch entries per thread at a time, loads first
+      for (int e0 = tid; e0 < na; e0 += kSpBatch * NT) {
+        E q[kSpBatch];
+        uint32_t bw[kSpBatch];
+        Real sv[kSpBatch];
+#pragma unroll
+        for (int u = 0; u < kSpBatch; ++u) q[u] = e0 + u * NT < na ? ea[e0 + u * NT] : E{Real(0), m};
+#pragma unroll
+        for (int u = 0; u < kSpBatch; ++u) {
+          bw[u] = bits_j[q[u].r >> 5];
+          sv[u] = slack[q[u].r];
+        }
+#pragma unroll
+        for (int u = 0; u < kSpBatch; ++u) {
+          const int e = e0 + u * NT;
+          if (e < na) {
+            Real w = Real(0);
+            if ((bw[u] >> (q[u].r & 31)) & 1u) w = eb[sp_lower_bound(eb, nb, q[u].r)].v;
+            const Real ae = T::pair_ae_r(q[u].v, w, cir, cjr);
+            pv[e] = ae;
+            T::acc(hi, lo, lo2, T::ratio(ae, sv[u]));
+          }
+        }
       }
       // rows of column j that column i does not hold; a shared row was taken
       // with column i's entry, and the marker (-0) makes this entry's update
       // a no-op below
-      for (int e = tid; e < nb; e += NT) {
-        const E q = eb[e];
-        Real ae = sp_mark(Real(0));
-        if (!((bits_i[q.r >> 5] >> (q.r & 31)) & 1u)) {
-          ae = T::pair_ae_r(Real(0), q.v, cir, cjr);
-          T::acc(hi, lo, lo2, T::ratio(ae, slack[q.r]));
+      for (int e0 = tid; e0 < nb; e0 += kSpBatch * NT) {
+        E q[kSpBatch];
+        uint32_t bw[kSpBatch];
+        Real sv[kSpBatch];
+#pragma unroll
+        for (int u = 0; u < kSpBatch; ++u) q[u] = e0 + u * NT < nb ? eb[e0 + u * NT] : E{Real(0), m};
+#pragma unroll
+        for (int u = 0; u < kSpBatch; ++u) {
+          bw[u] = bits_i[q[u].r >> 5];
+          sv[u] = slack[q[u].r];
         }
-        qv[e] = ae;
+#pragma unroll
+        for (int u = 0; u < kSpBatch; ++u) {
+          const int e = e0 + u * NT;
+          if (e < nb) {
+            Real ae = sp_mark(Real(0));
+            if (!((bw[u] >> (q[u].r & 31)) & 1u)) {
+              ae = T::pair_ae_r(Real(0), q[u].v, cir, cjr);
+              T::acc(hi, lo, lo2, T::ratio(ae, sv[u]));
+            }
+            qv[e] = ae;
+          }
+        }
       }
       // the update pass clears bits other threads tested: with more than one
       // warp the reduction's barrier orders the two, with one warp this
