@@ -221,6 +221,9 @@ def _compact(line):
     """The printed line: every section summarised so that the whole line stays
     near 3,000 characters (the full sections go to --detail-file)."""
     out = {k: line[k] for k in line if k not in _SECTIONS}
+    # the workload string already states the sizes
+    out["config"] = {k: v for k, v in line["config"].items()
+                     if k not in ("n", "d", "m", "chains", "samples_per_chain", "thinning", "pair_prob")}
     rf = dict(line["roofline"])
     for k in ("bytes_definition", "compressed_bytes_per_chr_step", "chr_steps_per_launch", "kernel_threads"):
         rf.pop(k, None)
@@ -276,9 +279,8 @@ def _compact(line):
         out["learned_rounding"] = {
             "train": lr["train"]["variants"], "test": lr["test_variants"],
             "mse": [_r(lr["test_mse_std_units"]), _r(lr["test_mse_mean_predictor"])],
-            "min_ess_s": {k: _r(v["min_ess_per_s_median"]) for k, v in lr["methods"].items()},
-            "rhat": {k: _r(v["rhat_max"]) for k, v in lr["methods"].items()},
-            "passed": {k: v["passed"] for k, v in lr["methods"].items()},
+            "min_ess_s,rhat,passed": {k: [_r(v["min_ess_per_s_median"]), _r(v["rhat_max"]), v["passed"]]
+                                      for k, v in lr["methods"].items()},
             **{k: _r(v, 3) for k, v in lr.items() if k.startswith("learned_vs_")}}
     return out
 

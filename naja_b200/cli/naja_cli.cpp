@@ -19,6 +19,10 @@
 //       the rows tight at the start (job_sampling.cu:196-235, T and shift
 //       composed as in :299-303); --extra-constraint-eps / --constraint-eps
 //       relax rows as job_sampling.cu:138-146 does.
+//   naja sample bulk --models-root DIR --model-list FILE --out-root DIR --name RUN --gpus 0,1,...
+//       src/cli/sample/cmd_bulk.cpp:20-163 and src/engine/job_bulk.cpp:115-267:
+//       every listed model sampled as `sample run` would, one host thread per
+//       GPU id, --skip-existing / --resume-from, bulk_summary.csv.
 //   naja sample calibrate-rounding --models-root DIR --model-list FILE --out F.csv
 //       src/cli/sample/cmd_calibrate_rounding.cpp:24-195: one pair schedule
 //       from warm-up moments pooled over a list of models.
@@ -31,10 +35,13 @@
 // The one flag value the reference accepts for a feature this project leaves
 // out (--start-policy cube_center, a Gurobi LP) is rejected with a usage
 // error instead of being ignored.
+#include <dirent.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
 #include <algorithm>
+#include <atomic>
+#include <cerrno>
 #include <charconv>
 #include <chrono>
 #include <cmath>
@@ -47,6 +54,7 @@
 #include <functional>
 #include <iomanip>
 #include <iostream>
+#include <mutex>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -186,23 +194,35 @@ std::vector<double> colmajor(const Csv& c) {
   return out;
 }
 
-// (rows, cols) float32 C order, header as src/npy.h:96-141 writes it.
-void save_npy_f32(const std::string& path, const float* data, long long rows, long long cols) {
+// One npy array, header padded as src/npy.h:56-79 / 96-141 pad it: the
+// header text is padded with spaces so that magic + version + length + text
+// reach a multiple of 64 bytes, then a newline.
+void save_npy_raw(const std::string& path, const char* descr, const std::string& shape, const void* data,
+                  size_t nbytes) {
   std::ofstream f(path, std::ios::binary);
   if (!f.is_open()) throw std::runtime_error("Cannot write file: " + path);
   f.write("\x93NUMPY", 6);
   f.put(0x01);
   f.put(0x00);
-  std::ostringstream h;
-  h << "{'descr': '<f4', 'fortran_order': False, 'shape': (" << rows << ", " << cols << "), }";
-  std::string hs = h.str();
+  std::string hs = std::string("{'descr': '") + descr + "', 'fortran_order': False, 'shape': (" + shape + "), }";
   const size_t total = 6 + 2 + 2 + hs.size();
   hs.append((64 - total % 64) % 64, ' ');
   hs.push_back('\n');
   const uint16_t len = static_cast<uint16_t>(hs.size());
   f.write(reinterpret_cast<const char*>(&len), 2);
   f.write(hs.data(), len);
-  f.write(reinterpret_cast<const char*>(data), static_cast<std::streamsize>(rows * cols * sizeof(float)));
+  f.write(reinterpret_cast<const char*>(data), static_cast<std::streamsize>(nbytes));
+}
+
+// (rows, cols) float32 C order (src/npy.h:96-141).
+void save_npy_f32(const std::string& path, const float* data, long long rows, long long cols) {
+  save_npy_raw(path, "<f4", std::to_string(rows) + ", " + std::to_string(cols), data,
+               static_cast<size_t>(rows * cols) * sizeof(float));
+}
+
+// 1-D uint8 (src/npy.h:56-79).
+void save_npy_u8(const std::string& path, const std::vector<uint8_t>& v) {
+  save_npy_raw(path, "|u1", std::to_string(v.size()) + ",", v.data(), v.size());
 }
 
 // Loads an npy of '<f4' or '<f8' as float32 (rows, cols) C order.
@@ -343,6 +363,9 @@ double seconds_since(std::chrono::steady_clock::time_point t0) {
             << "      [--backmap-mode fp64|tf32x3|bf16x3] [--verbose] [--quiet] [--dry-run] [--print-config]\n"
             << "      [--pair-schedule FILE] [--iter-rounding-passes P] [--iter-rounding-warmup W]\n"
             << "      [--affine-hull-tol t] [--extra-constraint-eps e] [--constraint-eps e]\n"
+            << "  naja sample bulk --models-root <dir> --model-list <file> --out-root <dir> --name <run>\n"
+            << "      --gpus <csv> --n-chains K --n-samples S [--skip-existing] [--resume-from <run_dir>]\n"
+            << "      [the per-job flags of sample run]\n"
             << "  naja sample calibrate-rounding --models-root <dir> --model-list <file> --out <csv>\n"
             << "      [--warmup 2000] [--passes 2] [--pair-prob 0.3] [--extra-constraint-eps 0] [--seed 1]\n"
             << "      [--max-models 0]\n";
@@ -441,12 +464,13 @@ void write_generated_config(const std::string& path, const RunConfig& c) {
     << "CONSTRAINT_EPS=" << c.constraint_eps << "\n";
 }
 
-void write_run_manifest(const RunConfig& c, const std::vector<std::string>& argv_full) {
+void write_run_manifest(const RunConfig& c, const std::vector<std::string>& argv_full,
+                        const std::string& name = "run_manifest.json") {
   const std::string exe = self_path();
   struct stat st {};
   stat(exe.c_str(), &st);
-  std::ofstream f(c.out_dir + "/run_manifest.json");
-  if (!f.is_open()) throw std::runtime_error("cannot write run manifest: " + c.out_dir + "/run_manifest.json");
+  std::ofstream f(c.out_dir + "/" + name);
+  if (!f.is_open()) throw std::runtime_error("cannot write run manifest: " + c.out_dir + "/" + name);
   f << "{\n  \"argv\": [";
   for (size_t i = 0; i < argv_full.size(); ++i) {
     if (i) f << ", ";
@@ -514,6 +538,134 @@ void write_config_used(const RunConfig& c, const std::string& gen) {
       << src.rdbuf() << "\n# Derived metadata\nMODEL_NAME=" << c.model_name << "\n"
       << "DATA_DIR_ABS=" << absolute(c.data_dir) << "\nMODEL_DIR_ABS=" << absolute(c.model_dir) << "\n"
       << "A_FILE=" << absolute(c.file("A")) << "\nB_FILE=" << absolute(c.file("b")) << "\n";
+}
+
+// GEM-bounds filter of the backmapped samples (src/engine/bounds_filter.cpp:
+// 65-180): sample j is valid when max over reactions i of
+// max((lb_i - x) - eps, (x - ub_i) - eps) is <= 0, x the float32 sample
+// widened to double.  Writes valid_mask.npy (uint8), valid_fraction.txt,
+// bounds_report.json (mean / p99 / max of the per-sample worst violation,
+// the ten reactions with the largest violation) and, if asked,
+// samples_valid.npy.  Samples are split over the host's cores; each thread
+// keeps its own per-reaction maxima, merged after the join (maxima, so the
+// result does not depend on the split).
+long long bounds_filter_and_write(const RunConfig& c, const std::vector<float>& out, long long N, long long dim) {
+  const std::string ids_path = c.gem_dir + "/reaction_ids.txt";
+  const std::string lb_path = c.gem_dir + "/l_bounds.csv", ub_path = c.gem_dir + "/u_bounds.csv";
+  require_nonempty(ids_path, "gem/reaction_ids.txt");
+  require_nonempty(lb_path, "gem/l_bounds.csv");
+  require_nonempty(ub_path, "gem/u_bounds.csv");
+  std::vector<std::string> ids;
+  {
+    std::ifstream f(ids_path);
+    for (std::string line; std::getline(f, line);) {
+      const size_t a = line.find_first_not_of(" \t\r\n"), z = line.find_last_not_of(" \t\r\n");
+      if (a != std::string::npos) ids.push_back(line.substr(a, z - a + 1));
+    }
+  }
+  const Csv l = load_csv(lb_path), u = load_csv(ub_path);
+  if (static_cast<long long>(ids.size()) != dim)
+    throw std::runtime_error("reaction_ids length mismatch: expected " + std::to_string(dim) + " got " +
+                             std::to_string(ids.size()));
+  if (static_cast<long long>(l.v.size()) != dim || static_cast<long long>(u.v.size()) != dim)
+    throw std::runtime_error("bounds length mismatch: expected " + std::to_string(dim) + " got lb=" +
+                             std::to_string(l.v.size()) + " ub=" + std::to_string(u.v.size()));
+  const double eps = c.bounds_eps;
+  std::vector<uint8_t> mask(static_cast<size_t>(N), 1);
+  std::vector<double> per_sample(static_cast<size_t>(N), 0.0);
+  const int nt = static_cast<int>(std::max<long long>(1, std::min<long long>(
+                     std::max(1u, std::thread::hardware_concurrency()), (N + 4095) / 4096)));
+  std::vector<std::vector<double>> worst_rxn(nt, std::vector<double>(static_cast<size_t>(dim), 0.0));
+  std::vector<double> worst_all(nt, 0.0);
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back([&, t] {
+      const long long j0 = N * t / nt, j1 = N * (t + 1) / nt;
+      double* wr = worst_rxn[t].data();
+      double wa = 0.0;
+      for (long long j = j0; j < j1; ++j) {
+        const float* x = out.data() + j * dim;
+        double worst = 0.0;
+        bool ok = true;
+        for (long long i = 0; i < dim; ++i) {
+          const double xi = x[i];
+          const double lo = (l.v[i] - xi) - eps, hi = (xi - u.v[i]) - eps;
+          const double v = lo > hi ? lo : hi;
+          if (v > 0.0) {
+            ok = false;
+            if (v > wa) wa = v;
+            if (v > wr[i]) wr[i] = v;
+            if (v > worst) worst = v;
+          }
+        }
+        mask[j] = ok ? 1 : 0;
+        per_sample[j] = worst;
+      }
+      worst_all[t] = wa;
+    });
+  for (auto& th : pool) th.join();
+  double max_violation = 0.0;
+  std::vector<double> by_rxn(static_cast<size_t>(dim), 0.0);
+  for (int t = 0; t < nt; ++t) {
+    max_violation = std::max(max_violation, worst_all[t]);
+    for (long long i = 0; i < dim; ++i) by_rxn[i] = std::max(by_rxn[i], worst_rxn[t][i]);
+  }
+  long long n_valid = 0;
+  for (uint8_t m : mask) n_valid += m != 0;
+  save_npy_u8(c.out_dir + "/valid_mask.npy", mask);
+  {
+    std::ofstream vf(c.out_dir + "/valid_fraction.txt");
+    if (!vf.is_open()) throw std::runtime_error("cannot write valid_fraction.txt");
+    vf << std::setprecision(12) << (N ? static_cast<double>(n_valid) / static_cast<double>(N) : 0.0) << "\n";
+  }
+  if (c.write_samples_valid) {
+    std::vector<float> valid;
+    valid.reserve(static_cast<size_t>(n_valid * dim));
+    for (long long j = 0; j < N; ++j)
+      if (mask[j]) valid.insert(valid.end(), out.data() + j * dim, out.data() + (j + 1) * dim);
+    save_npy_f32(c.out_dir + "/samples_valid.npy", valid.data(), n_valid, dim);
+  }
+  double mean_v = 0.0;
+  for (double v : per_sample) mean_v += v;
+  mean_v = N ? mean_v / static_cast<double>(N) : 0.0;
+  double p99 = 0.0;
+  if (N > 0) {
+    const size_t k = static_cast<size_t>((99 * (N - 1)) / 100);
+    std::nth_element(per_sample.begin(), per_sample.begin() + static_cast<std::ptrdiff_t>(k), per_sample.end());
+    p99 = per_sample[k];
+  }
+  std::vector<std::pair<long long, double>> top;
+  for (long long i = 0; i < dim; ++i) top.emplace_back(i, by_rxn[i]);
+  const size_t k_top = static_cast<size_t>(std::min<long long>(dim, 10));
+  std::partial_sort(top.begin(), top.begin() + static_cast<std::ptrdiff_t>(k_top), top.end(),
+                    [](const auto& a, const auto& b) { return a.second > b.second; });
+  top.resize(k_top);
+  while (!top.empty() && top.back().second <= 0.0) top.pop_back();
+  std::ofstream f(c.out_dir + "/bounds_report.json");
+  if (!f.is_open()) throw std::runtime_error("Cannot write bounds report: " + c.out_dir + "/bounds_report.json");
+  f << std::setprecision(12) << "{\n  \"model\": ";
+  json_string(f, c.model_name);
+  f << ",\n  \"model_dir\": ";
+  json_string(f, absolute(c.model_dir));
+  f << ",\n  \"run_dir\": ";
+  json_string(f, absolute(c.out_dir));
+  f << ",\n  \"eps\": " << eps << ",\n  \"n_total\": " << N << ",\n  \"n_valid\": " << n_valid
+    << ",\n  \"n_invalid\": " << (N - n_valid) << ",\n  \"invalid_fraction\": "
+    << (N ? static_cast<double>(N - n_valid) / static_cast<double>(N) : 0.0) << ",\n  \"mean_violation\": " << mean_v
+    << ",\n  \"p99_violation\": " << p99 << ",\n  \"max_violation\": " << max_violation
+    << ",\n  \"outputs\": {\n    \"valid_mask\": ";
+  json_string(f, absolute(c.out_dir + "/valid_mask.npy"));
+  f << ",\n    \"samples_valid\": ";
+  if (c.write_samples_valid) json_string(f, absolute(c.out_dir + "/samples_valid.npy"));
+  else f << "null";
+  f << "\n  },\n  \"top_violations\": [\n";
+  for (size_t i = 0; i < top.size(); ++i) {
+    f << "    {\"index\": " << top[i].first << ", \"reaction\": ";
+    json_string(f, ids[static_cast<size_t>(top[i].first)]);
+    f << ", \"worst_violation\": " << top[i].second << "}" << (i + 1 != top.size() ? "," : "") << "\n";
+  }
+  f << "  ]\n}\n";
+  return n_valid;
 }
 
 int run_sampling(const RunConfig& c) {
@@ -720,25 +872,8 @@ int run_sampling(const RunConfig& c) {
   }
   if (c.bounds_policy == "filter") {
     phase(st, "bounds filter (GEM validity)");
-    const Csv l = load_csv(c.gem_dir + "/l_bounds.csv"), u = load_csv(c.gem_dir + "/u_bounds.csv");
-    if (static_cast<long long>(l.v.size()) != dim || static_cast<long long>(u.v.size()) != dim)
-      throw std::runtime_error("GEM bounds length does not match the sample dimension");
-    std::vector<float> valid;
-    long long n_ok = 0;
-    for (long long s = 0; s < N; ++s) {
-      const float* v = out.data() + s * dim;
-      bool ok = true;
-      for (long long i = 0; i < dim && ok; ++i) {
-        const double viol = std::max(l.v[i] - v[i], v[i] - u.v[i]);
-        if (viol - c.bounds_eps > 0.0) ok = false;
-      }
-      if (ok) {
-        ++n_ok;
-        if (c.write_samples_valid) valid.insert(valid.end(), v, v + dim);
-      }
-    }
+    const long long n_ok = bounds_filter_and_write(c, out, N, dim);
     kv(st, "bounds_valid", std::to_string(n_ok) + "/" + std::to_string(N));
-    if (c.write_samples_valid) save_npy_f32(c.out_dir + "/samples_valid.npy", valid.data(), n_ok, dim);
   }
   prof.total = seconds_since(t_total);
   write_profile(c.out_dir + "/profile.json", prof, c);
@@ -747,50 +882,47 @@ int run_sampling(const RunConfig& c) {
   return 0;
 }
 
-int cmd_sample_run(int argc, char** argv) {
-  RunConfig c;
-  std::string out_root;
-  for (int i = 0; i < argc; ++i) {
-    const std::string a = argv[i];
-    if (a == "--model-dir") c.model_dir = next_arg(i, argc, argv, a);
-    else if (a == "--out-root") out_root = next_arg(i, argc, argv, a);
-    else if (a == "--gpu") c.gpu = std::stoi(next_arg(i, argc, argv, a));
-    else if (a == "--n-chains") c.n_chains = std::stoi(next_arg(i, argc, argv, a));
-    else if (a == "--n-samples") c.n_samples = std::stoi(next_arg(i, argc, argv, a));
-    else if (a == "--tpb") {
-      c.tpb = std::stoi(next_arg(i, argc, argv, a));
-      c.tpb_set = true;
-    }
-    else if (a == "--thinning") c.thinning = std::stoi(next_arg(i, argc, argv, a));
-    else if (a == "--pair-prob") c.pair_prob = std::stod(next_arg(i, argc, argv, a));
-    else if (a == "--resync-interval") c.resync_interval = std::stoi(next_arg(i, argc, argv, a));
-    else if (a == "--ksparse-prob") c.ksparse_prob = std::stod(next_arg(i, argc, argv, a));
-    else if (a == "--ksparse-k") c.ksparse_k = std::stoi(next_arg(i, argc, argv, a));
-    else if (a == "--extra-constraints") c.extra_constraints = next_arg(i, argc, argv, a);
-    else if (a == "--backmap") c.backmap = true;
-    else if (a == "--write-npy") c.write_npy = true;
-    else if (a == "--verbose") c.verbose = true;
-    else if (a == "--bounds-policy") c.bounds_policy = next_arg(i, argc, argv, a);
-    else if (a == "--bounds-eps") c.bounds_eps = std::stod(next_arg(i, argc, argv, a));
-    else if (a == "--write-samples-valid") c.write_samples_valid = true;
-    else if (a == "--quiet") c.quiet = true;
-    else if (a == "--dry-run") c.dry_run = true;
-    else if (a == "--print-config") c.print_config = true;
-    else if (a == "--precision") c.precision = next_arg(i, argc, argv, a);
-    else if (a == "--rng") c.rng = next_arg(i, argc, argv, a);
-    else if (a == "--backmap-mode") c.backmap_mode = next_arg(i, argc, argv, a);
-    else if (a == "--start-policy") {
-      if (next_arg(i, argc, argv, a) != "file") die_usage("invalid --start-policy (only 'file' is supported)");
-    } else if (a == "--iter-rounding-passes") c.iter_rounding_passes = std::stoi(next_arg(i, argc, argv, a));
-    else if (a == "--iter-rounding-warmup") c.iter_rounding_warmup = std::stoi(next_arg(i, argc, argv, a));
-    else if (a == "--pair-schedule" || a == "--pair-schedule-file") c.pair_schedule = next_arg(i, argc, argv, a);
-    else if (a == "--affine-hull-tol") c.affine_hull_tol = std::stod(next_arg(i, argc, argv, a));
-    else if (a == "--extra-constraint-eps") c.extra_constraint_eps = std::stod(next_arg(i, argc, argv, a));
-    else if (a == "--constraint-eps") c.constraint_eps = std::stod(next_arg(i, argc, argv, a));
-    else die_usage("unknown flag: " + a);
+// The per-job flags shared by `sample run` and `sample bulk`
+// (src/cli/sample/cmd_run.cpp:44-120, cmd_bulk.cpp:41-64).  Returns false
+// for a flag that is not one of them.
+bool parse_job_flag(RunConfig& c, const std::string& a, int& i, int argc, char** argv) {
+  if (a == "--n-chains") c.n_chains = std::stoi(next_arg(i, argc, argv, a));
+  else if (a == "--n-samples") c.n_samples = std::stoi(next_arg(i, argc, argv, a));
+  else if (a == "--tpb") {
+    c.tpb = std::stoi(next_arg(i, argc, argv, a));
+    c.tpb_set = true;
   }
-  if (c.model_dir.empty()) die_usage("missing --model-dir");
-  if (out_root.empty()) die_usage("missing --out-root");
+  else if (a == "--thinning") c.thinning = std::stoi(next_arg(i, argc, argv, a));
+  else if (a == "--pair-prob") c.pair_prob = std::stod(next_arg(i, argc, argv, a));
+  else if (a == "--resync-interval") c.resync_interval = std::stoi(next_arg(i, argc, argv, a));
+  else if (a == "--ksparse-prob") c.ksparse_prob = std::stod(next_arg(i, argc, argv, a));
+  else if (a == "--ksparse-k") c.ksparse_k = std::stoi(next_arg(i, argc, argv, a));
+  else if (a == "--extra-constraints") c.extra_constraints = next_arg(i, argc, argv, a);
+  else if (a == "--backmap") c.backmap = true;
+  else if (a == "--write-npy") c.write_npy = true;
+  else if (a == "--verbose") c.verbose = true;
+  else if (a == "--bounds-policy") c.bounds_policy = next_arg(i, argc, argv, a);
+  else if (a == "--bounds-eps") c.bounds_eps = std::stod(next_arg(i, argc, argv, a));
+  else if (a == "--write-samples-valid") c.write_samples_valid = true;
+  else if (a == "--quiet") c.quiet = true;
+  else if (a == "--dry-run") c.dry_run = true;
+  else if (a == "--print-config") c.print_config = true;
+  else if (a == "--precision") c.precision = next_arg(i, argc, argv, a);
+  else if (a == "--rng") c.rng = next_arg(i, argc, argv, a);
+  else if (a == "--backmap-mode") c.backmap_mode = next_arg(i, argc, argv, a);
+  else if (a == "--start-policy") {
+    if (next_arg(i, argc, argv, a) != "file") die_usage("invalid --start-policy (only 'file' is supported)");
+  } else if (a == "--iter-rounding-passes") c.iter_rounding_passes = std::stoi(next_arg(i, argc, argv, a));
+  else if (a == "--iter-rounding-warmup") c.iter_rounding_warmup = std::stoi(next_arg(i, argc, argv, a));
+  else if (a == "--pair-schedule" || a == "--pair-schedule-file") c.pair_schedule = next_arg(i, argc, argv, a);
+  else if (a == "--affine-hull-tol") c.affine_hull_tol = std::stod(next_arg(i, argc, argv, a));
+  else if (a == "--extra-constraint-eps") c.extra_constraint_eps = std::stod(next_arg(i, argc, argv, a));
+  else if (a == "--constraint-eps") c.constraint_eps = std::stod(next_arg(i, argc, argv, a));
+  else return false;
+  return true;
+}
+
+void check_job_flags(const RunConfig& c) {
   if (c.n_chains <= 0) die_usage("invalid --n-chains");
   if (c.n_samples <= 0) die_usage("invalid --n-samples");
   if (c.pair_prob < 0.0 || c.pair_prob > 1.0) die_usage("invalid --pair-prob (must be in [0,1])");
@@ -810,8 +942,10 @@ int cmd_sample_run(int argc, char** argv) {
   if (c.backmap_mode != "fp64" && c.backmap_mode != "tf32x3" && c.backmap_mode != "bf16x3")
     die_usage("invalid --backmap-mode (fp64|tf32x3|bf16x3)");
   if (c.bounds_policy == "filter" && !c.backmap) throw std::runtime_error("bounds-policy=filter requires --backmap");
+}
 
-  std::string md = c.model_dir;
+// Model name and contract paths of a model directory (model_contract.cpp:56-84).
+void set_model(RunConfig& c, std::string md) {
   if (!md.empty() && md.back() == '/') md.pop_back();
   if (!is_directory(md)) throw std::runtime_error("model-dir is not a directory: " + md);
   const auto slash = md.find_last_of('/');
@@ -820,6 +954,22 @@ int cmd_sample_run(int argc, char** argv) {
   c.rounding_dir = md + "/rounding";
   c.gem_dir = md + "/gem";
   c.data_dir = slash == std::string::npos ? "." : md.substr(0, slash);
+}
+
+int cmd_sample_run(int argc, char** argv) {
+  RunConfig c;
+  std::string out_root;
+  for (int i = 0; i < argc; ++i) {
+    const std::string a = argv[i];
+    if (a == "--model-dir") c.model_dir = next_arg(i, argc, argv, a);
+    else if (a == "--out-root") out_root = next_arg(i, argc, argv, a);
+    else if (a == "--gpu") c.gpu = std::stoi(next_arg(i, argc, argv, a));
+    else if (!parse_job_flag(c, a, i, argc, argv)) die_usage("unknown flag: " + a);
+  }
+  if (c.model_dir.empty()) die_usage("missing --model-dir");
+  if (out_root.empty()) die_usage("missing --out-root");
+  check_job_flags(c);
+  set_model(c, c.model_dir);
   validate_contract(c);
   c.out_dir = allocate_run_dir(out_root, c.model_name);
   const bool st = !c.quiet;
@@ -1000,6 +1150,242 @@ int cmd_calibrate_rounding(int argc, char** argv) {
   return 0;
 }
 
+// ------------------------------------------------------------ sample bulk
+// Every model of a list sampled into one run directory
+// (src/cli/sample/cmd_bulk.cpp:20-163, src/engine/job_bulk.cpp:115-267):
+// one host thread per entry of --gpus, all pulling the next model index
+// from one atomic counter; each job gets <run>/<model>/<model>_<date>_<NNN>
+// and runs exactly as `sample run` would (same flags, seed from model name,
+// model directory and GPU).  --skip-existing takes a model as done when a
+// job directory of it holds a non-empty samples.npy and profile.json (and,
+// with the bounds filter, valid_mask.npy, valid_fraction.txt and
+// bounds_report.json); --resume-from reuses a run directory.  The run ends
+// with bulk_summary.csv (model,status,elapsed_s,device_id,message,
+// output_dir,inherited_from_base) and fails when any job failed.
+struct BulkResult {
+  std::string model, status, message, output_dir;
+  double elapsed = 0.0;
+  int device = 0;
+};
+
+bool file_nonempty(const std::string& path) {
+  struct stat st;
+  return stat(path.c_str(), &st) == 0 && st.st_size > 0;
+}
+
+std::vector<int> parse_gpu_list(const std::string& s) {
+  std::vector<int> ids;
+  std::stringstream ss(s);
+  for (std::string tok; std::getline(ss, tok, ',');) {
+    const size_t a = tok.find_first_not_of(" \t"), z = tok.find_last_not_of(" \t");
+    if (a == std::string::npos) continue;
+    const std::string t = tok.substr(a, z - a + 1);
+    int id = -1;
+    const auto [end, ec] = std::from_chars(t.data(), t.data() + t.size(), id);
+    if (ec != std::errc() || end != t.data() + t.size() || id < 0) die_usage("invalid --gpus entry: " + t);
+    ids.push_back(id);
+  }
+  if (ids.empty()) die_usage("invalid --gpus: " + s);
+  return ids;
+}
+
+// The newest job directory of `model` under the run directory with complete
+// outputs (job_bulk.cpp:86-111), or "".
+std::string find_completed_job_dir(const std::string& run_dir, const std::string& model, bool filter) {
+  const std::string root = run_dir + "/" + model;
+  DIR* d = opendir(root.c_str());
+  if (!d) return {};
+  std::string best;
+  time_t best_mtime = 0;
+  for (dirent* e; (e = readdir(d)) != nullptr;) {
+    const std::string name = e->d_name;
+    if (name == "." || name == "..") continue;
+    const std::string dir = root + "/" + name;
+    struct stat st;
+    if (stat(dir.c_str(), &st) != 0 || !S_ISDIR(st.st_mode)) continue;
+    if (!file_nonempty(dir + "/samples.npy") || !file_nonempty(dir + "/profile.json")) continue;
+    if (filter && (!file_nonempty(dir + "/valid_mask.npy") || !file_nonempty(dir + "/valid_fraction.txt") ||
+                   !file_nonempty(dir + "/bounds_report.json")))
+      continue;
+    if (best.empty() || st.st_mtime > best_mtime) {
+      best = dir;
+      best_mtime = st.st_mtime;
+    }
+  }
+  closedir(d);
+  return best;
+}
+
+// <root>/<model>_<YYYYMMDD>_<NNN>, claimed by mkdir itself so that two
+// workers given the same model never share a directory.
+std::string claim_job_dir(const std::string& root, const std::string& model) {
+  ensure_dir(root);
+  const std::string date = stamp("%Y%m%d");
+  for (int idx = 1; idx < 1000000; ++idx) {
+    std::ostringstream o;
+    o << root << "/" << model << "_" << date << "_" << std::setw(3) << std::setfill('0') << idx;
+    if (mkdir(o.str().c_str(), 0755) == 0) return o.str();
+    if (errno != EEXIST) throw std::runtime_error("cannot create directory: " + o.str());
+  }
+  throw std::runtime_error("could not allocate job directory under " + root);
+}
+
+std::string inherited_from_base(const std::string& models_root, const std::string& model) {
+  std::ifstream f(models_root + "/" + model + "/rounding/INHERITED_FROM.txt");
+  for (std::string line; std::getline(f, line);) {
+    const size_t a = line.find_first_not_of(" \t\r\n"), z = line.find_last_not_of(" \t\r\n");
+    if (a == std::string::npos) continue;
+    line = line.substr(a, z - a + 1);
+    if (line.rfind("base_model_dir=", 0) == 0) return line.substr(15);
+  }
+  return {};
+}
+
+int cmd_sample_bulk(int argc, char** argv) {
+  RunConfig base;
+  std::string models_root, model_list, out_root, resume_from, name, gpus;
+  bool skip_existing = false;
+  for (int i = 0; i < argc; ++i) {
+    const std::string a = argv[i];
+    if (a == "--models-root") models_root = next_arg(i, argc, argv, a);
+    else if (a == "--model-list") model_list = next_arg(i, argc, argv, a);
+    else if (a == "--out-root") out_root = next_arg(i, argc, argv, a);
+    else if (a == "--resume-from") resume_from = next_arg(i, argc, argv, a);
+    else if (a == "--name") name = next_arg(i, argc, argv, a);
+    else if (a == "--gpus") gpus = next_arg(i, argc, argv, a);
+    else if (a == "--skip-existing") skip_existing = true;
+    else if (!parse_job_flag(base, a, i, argc, argv)) die_usage("unknown flag: " + a);
+  }
+  if (models_root.empty()) die_usage("missing --models-root");
+  if (model_list.empty()) die_usage("missing --model-list");
+  if (name.empty()) die_usage("missing --name");
+  if (gpus.empty()) die_usage("missing --gpus");
+  check_job_flags(base);
+  const std::vector<int> gpu_ids = parse_gpu_list(gpus);
+  if (!is_directory(models_root)) throw std::runtime_error("models-root is not a directory: " + models_root);
+  const std::vector<std::string> models = load_model_list(model_list);
+  std::vector<RunConfig> jobs;
+  for (const auto& m : models) {
+    RunConfig jc = base;
+    set_model(jc, models_root + "/" + m);
+    validate_contract(jc);
+    jobs.push_back(std::move(jc));
+  }
+  RunConfig run = base;
+  run.model_dir = models_root;
+  run.data_dir = models_root;
+  run.model_name = name;
+  if (!resume_from.empty()) {
+    if (!is_directory(resume_from)) throw std::runtime_error("resume-from is not a directory: " + resume_from);
+    run.out_dir = resume_from;
+  } else {
+    if (out_root.empty()) die_usage("missing --out-root (or use --resume-from)");
+    run.out_dir = allocate_run_dir(out_root, name);
+  }
+  const bool st = !base.quiet;
+  phase(st, "validate model contracts");
+  phase(st, "write generated bulk config");
+  const std::string gen = run.out_dir + "/bulk_config_generated.txt";
+  write_generated_config(gen, run);
+  {
+    std::ofstream f(gen, std::ios::app);
+    f << "GPU_LIST=" << gpus << "\nBULK_MODEL_LIST=" << model_list << "\nSKIP_EXISTING=" << (skip_existing ? 1 : 0)
+      << "\n";
+  }
+  if (base.print_config) {
+    std::cout << "config_generated    :: " << absolute(gen) << "\n---\n";
+    std::ifstream f(gen);
+    std::cout << f.rdbuf() << "---\n";
+  }
+  std::vector<std::string> full = {"naja", "sample", "bulk"};
+  for (int i = 0; i < argc; ++i) full.push_back(argv[i]);
+  const bool resumed = !resume_from.empty() && path_exists(run.out_dir + "/run_manifest.json");
+  write_run_manifest(run, full, resumed ? "run_manifest_resume.json" : "run_manifest.json");
+  kv(st, "bulk_name", name);
+  kv(st, "jobs", std::to_string(jobs.size()));
+  kv(st, "gpus", gpus);
+  kv(st, "output", absolute(run.out_dir));
+  kv(st, "bounds", base.bounds_policy);
+  if (base.bounds_policy == "filter") kv(st, "bounds_eps", std::to_string(base.bounds_eps));
+  if (skip_existing) kv(st, "skip_existing", "true");
+  if (base.dry_run) {
+    phase(st, "dry-run: not executing bulk sampling");
+    return 0;
+  }
+  phase(st, "bulk sampling");
+  std::cout << "bulk sampling :: " << jobs.size() << " jobs across " << gpu_ids.size() << " gpu(s)\n"
+            << "output root   :: " << absolute(run.out_dir) << "\n" << std::endl;
+
+  std::atomic<size_t> next{0};
+  std::mutex mu;
+  std::vector<BulkResult> results;
+  const bool filter = base.bounds_policy == "filter";
+  auto worker = [&](int device) {
+    for (;;) {
+      const size_t k = next.fetch_add(1);
+      if (k >= jobs.size()) return;
+      RunConfig jc = jobs[k];
+      jc.gpu = device;
+      jc.quiet = true;
+      jc.print_config = false;
+      BulkResult r;
+      r.model = jc.model_name;
+      r.device = device;
+      const auto t0 = std::chrono::steady_clock::now();
+      std::string done = skip_existing ? find_completed_job_dir(run.out_dir, jc.model_name, filter) : std::string();
+      if (!done.empty()) {
+        r.status = "SKIP";
+        r.message = "SKIP";
+        r.output_dir = done;
+      } else {
+        try {
+          jc.out_dir = claim_job_dir(run.out_dir + "/" + jc.model_name, jc.model_name);
+          r.output_dir = jc.out_dir;
+          write_generated_config(jc.out_dir + "/config_generated.txt", jc);
+          const int rc = run_sampling(jc);
+          r.status = rc == 0 ? "OK" : "FAIL";
+          if (rc != 0) r.message = "return code " + std::to_string(rc);
+        } catch (const std::exception& e) {
+          r.status = "FAIL";
+          r.message = e.what();
+        }
+        r.elapsed = seconds_since(t0);
+      }
+      std::lock_guard<std::mutex> lock(mu);
+      std::cout << "[gpu " << device << "] " << r.model << " -> " << r.status;
+      if (r.status != "SKIP") {
+        std::cout << " (" << std::fixed << std::setprecision(2) << r.elapsed << "s";
+        if (r.status == "FAIL" && !r.message.empty()) std::cout << ", " << r.message;
+        std::cout << ")";
+      }
+      std::cout << std::endl;
+      results.push_back(std::move(r));
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int id : gpu_ids) pool.emplace_back(worker, id);
+  for (auto& t : pool) t.join();
+
+  size_t ok = 0;
+  for (const auto& r : results) ok += r.status != "FAIL";
+  std::cout << "\nsummary\n  completed : " << ok << " / " << jobs.size() << "\n" << std::endl;
+  const std::string summary = run.out_dir + "/bulk_summary.csv";
+  std::ofstream f(summary);
+  if (!f.is_open()) throw std::runtime_error("cannot write bulk summary: " + summary);
+  f << "model,status,elapsed_s,device_id,message,output_dir,inherited_from_base\n";
+  for (const auto& r : results) {
+    std::string msg = r.message;
+    std::replace(msg.begin(), msg.end(), '\n', ' ');
+    f << r.model << "," << r.status << "," << std::fixed << std::setprecision(2) << r.elapsed << "," << r.device
+      << "," << msg << "," << r.output_dir << "," << inherited_from_base(models_root, r.model) << "\n";
+  }
+  f.close();
+  std::cout << "  wrote summary :: " << summary << std::endl;
+  if (ok != jobs.size()) throw std::runtime_error("bulk sampling failed with return code 2");
+  return 0;
+}
+
+
 // ------------------------------------------------------------ validate
 float percentile(std::vector<float> v, float q) {
   if (v.empty()) return 0.0f;
@@ -1150,6 +1536,8 @@ int main(int argc, char** argv) {
   try {
     if (argc >= 3 && std::string(argv[1]) == "sample" && std::string(argv[2]) == "run")
       return cmd_sample_run(argc - 3, argv + 3);
+    if (argc >= 3 && std::string(argv[1]) == "sample" && std::string(argv[2]) == "bulk")
+      return cmd_sample_bulk(argc - 3, argv + 3);
     if (argc >= 3 && std::string(argv[1]) == "sample" && std::string(argv[2]) == "calibrate-rounding")
       return cmd_calibrate_rounding(argc - 3, argv + 3);
     if (argc >= 2 && std::string(argv[1]) == "validate") return cmd_validate(argc - 2, argv + 2);
@@ -1158,6 +1546,8 @@ int main(int argc, char** argv) {
       return 0;
     }
     std::cerr << "usage:\n  naja sample run --model-dir <dir> --out-root <dir> --n-chains K --n-samples S [...]\n"
+              << "  naja sample bulk --models-root <dir> --model-list <file> --out-root <dir> --name <run> --gpus <csv>\n"
+              << "      --n-chains K --n-samples S [--skip-existing] [--resume-from <run_dir>] [...]\n"
               << "  naja sample calibrate-rounding --models-root <dir> --model-list <file> --out <csv> [...]\n"
               << "  naja validate --samples <file.npy> [--model-dir <dir>] [--n-chains 4]\n  naja version\n";
     return 2;

@@ -89,3 +89,56 @@ def test_usage_errors(tmp_path):
     r = _run(*base, "--n-chains", 1, "--n-samples", 1, "--bounds-policy", "filter")
     assert r.returncode == 1 and "requires --backmap" in r.stderr
     assert _run("validate").returncode == 2
+
+
+def _bulk_models(tmp, names=("M1", "M2")):
+    for n in names:
+        _model(tmp, n)
+    lst = tmp / "models.txt"
+    lst.write_text("# models\n" + "\n".join(names) + "\n\n")
+    return tmp / "models", lst
+
+
+def test_bulk_dry_run_files(tmp_path):
+    root, lst = _bulk_models(tmp_path)
+    r = _run("sample", "bulk", "--models-root", root, "--model-list", lst, "--out-root", tmp_path / "out",
+             "--name", "RUN", "--gpus", "0,1", "--n-chains", 2, "--n-samples", 3, "--dry-run")
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.splitlines()
+    for want in ("> validate model contracts", "> write generated bulk config", "> dry-run: not executing bulk sampling"):
+        assert want in lines
+    runs = list((tmp_path / "out").iterdir())
+    assert len(runs) == 1 and runs[0].name.startswith("RUN_") and runs[0].name.endswith("_001")
+    cfg = (runs[0] / "bulk_config_generated.txt").read_text()
+    assert "GPU_LIST=0,1" in cfg and f"BULK_MODEL_LIST={lst}" in cfg and "N_CHAINS=2" in cfg
+    man = json.loads((runs[0] / "run_manifest.json").read_text())
+    assert man["argv"][:3] == ["naja", "sample", "bulk"]
+    # resuming into the same run directory writes the resume manifest beside the first
+    r = _run("sample", "bulk", "--models-root", root, "--model-list", lst, "--resume-from", runs[0], "--name", "RUN",
+             "--gpus", "0", "--n-chains", 2, "--n-samples", 3, "--dry-run", "--skip-existing")
+    assert r.returncode == 0, r.stderr
+    assert (runs[0] / "run_manifest_resume.json").exists()
+    lines = r.stdout.splitlines()
+    assert "  jobs            2" in lines and "  skip_existing   true" in lines
+
+
+def test_bulk_usage_and_contract_errors(tmp_path):
+    root, lst = _bulk_models(tmp_path)
+    base = ["sample", "bulk", "--models-root", root, "--model-list", lst, "--out-root", tmp_path / "out",
+            "--name", "RUN", "--n-chains", 1, "--n-samples", 1, "--dry-run"]
+    assert _run(*base).returncode == 2  # missing --gpus
+    assert _run(*base, "--gpus", "x").returncode == 2
+    assert _run(*base, "--gpus", "0", "--bogus").returncode == 2
+    r = _run("sample", "bulk", "--models-root", root, "--model-list", lst, "--name", "RUN", "--gpus", "0",
+             "--n-chains", 1, "--n-samples", 1, "--dry-run")
+    assert r.returncode == 2 and "--out-root" in r.stderr
+    # every model's contract is checked before anything runs
+    (root / "M2" / "rounding" / "M2_rounding_b.csv").write_text("")
+    r = _run(*base, "--gpus", "0")
+    assert r.returncode == 1 and "empty rounding_b" in r.stderr
+    assert not (tmp_path / "out").exists()
+    empty = tmp_path / "empty.txt"
+    empty.write_text("# nothing\n")
+    r = _run("sample", "bulk", "--models-root", root, "--model-list", empty, "--out-root", tmp_path / "out",
+             "--name", "RUN", "--gpus", "0", "--n-chains", 1, "--n-samples", 1, "--dry-run")
+    assert r.returncode == 1

@@ -29,22 +29,23 @@ def _write(path, M):
     np.savetxt(path, M, delimiter=",", fmt="%.17g")
 
 
-def _model_dir(tmp):
+def _model_dir(tmp, name="G130", seed=3):
     g = synth.genome_shaped(n=130, d=40, density=0.1, seed_T=7, seed_u=8)
-    v = synth.conditioned_variants(g, 1, max_reactions=10, seed=3)[0]
-    md = tmp / "models" / "G130"
+    v = synth.conditioned_variants(g, 1, max_reactions=10, seed=seed)[0]
+    md = tmp / "models" / name
     (md / "rounding").mkdir(parents=True)
     (md / "gem").mkdir()
     r = md / "rounding"
-    _write(r / "G130_rounding_A.csv", g["A"])
-    _write(r / "G130_rounding_b.csv", g["b"].reshape(-1, 1))
-    _write(r / "G130_rounding_start.csv", g["start"].reshape(-1, 1))
-    _write(r / "G130_rounding_T.csv", g["T"])
-    _write(r / "G130_rounding_shift.csv", g["shift"].reshape(-1, 1))
-    _write(r / "G130_rounding_extra_A.csv", v["extra_A"])
-    _write(r / "G130_rounding_extra_b.csv", v["extra_b"].reshape(-1, 1))
+    _write(r / f"{name}_rounding_A.csv", g["A"])
+    _write(r / f"{name}_rounding_b.csv", g["b"].reshape(-1, 1))
+    _write(r / f"{name}_rounding_start.csv", g["start"].reshape(-1, 1))
+    _write(r / f"{name}_rounding_T.csv", g["T"])
+    _write(r / f"{name}_rounding_shift.csv", g["shift"].reshape(-1, 1))
+    _write(r / f"{name}_rounding_extra_A.csv", v["extra_A"])
+    _write(r / f"{name}_rounding_extra_b.csv", v["extra_b"].reshape(-1, 1))
     _write(md / "gem" / "l_bounds.csv", v["l_new"].reshape(-1, 1))
     _write(md / "gem" / "u_bounds.csv", v["u_new"].reshape(-1, 1))
+    (md / "gem" / "reaction_ids.txt").write_text("".join(f"R_{k}\n" for k in range(130)))
     A = np.vstack([g["A"], v["extra_A"]])
     b = np.concatenate([g["b"], v["extra_b"]])
     return md, A, b
@@ -102,6 +103,87 @@ def test_backmap_bounds_filter(cuda, tmp_path):
     assert rep["bounds"]["n_checked"] == 200 * 130
     # the same rule as the filter: no violating pair exactly when every sample was kept
     assert (rep["bounds"]["n_violations"] == 0) == (valid.shape[0] == 200)
+    _check_filter_outputs(run, md, V_, 1e-6)
+
+
+def _check_filter_outputs(run, md, V_, eps):
+    """valid_mask.npy / valid_fraction.txt / bounds_report.json as
+    src/engine/bounds_filter.cpp:65-180 writes them, recomputed here."""
+    lb = np.loadtxt(md / "gem" / "l_bounds.csv", delimiter=",").reshape(-1)
+    ub = np.loadtxt(md / "gem" / "u_bounds.csv", delimiter=",").reshape(-1)
+    x = V_.astype(np.float64)
+    viol = np.maximum((lb - x) - eps, (x - ub) - eps)
+    worst = np.where(viol > 0, viol, 0.0).max(axis=1)
+    mask = np.load(run / "valid_mask.npy")
+    assert mask.dtype == np.uint8 and mask.shape == (V_.shape[0],)
+    assert np.array_equal(mask, (worst == 0).astype(np.uint8))
+    assert float((run / "valid_fraction.txt").read_text()) == pytest.approx(mask.mean(), rel=1e-11)
+    valid = np.load(run / "samples_valid.npy")
+    assert np.array_equal(valid, V_[mask == 1])
+    rep = json.loads((run / "bounds_report.json").read_text())
+    assert rep["n_total"] == V_.shape[0] and rep["n_valid"] == int(mask.sum())
+    assert rep["max_violation"] == pytest.approx(worst.max(), rel=1e-11, abs=0)
+    assert rep["mean_violation"] == pytest.approx(worst.mean(), rel=1e-9, abs=1e-300)
+    assert rep["p99_violation"] == pytest.approx(np.sort(worst)[(99 * (len(worst) - 1)) // 100], rel=1e-11, abs=0)
+    by_rxn = np.where(viol > 0, viol, 0.0).max(axis=0)
+    top = [t["index"] for t in rep["top_violations"]]
+    want = [int(k) for k in np.argsort(-by_rxn, kind="stable")[:10] if by_rxn[k] > 0]
+    assert sorted(top) == sorted(want)
+    assert all(t["reaction"] == f"R_{t['index']}" for t in rep["top_violations"])
+    assert rep["outputs"]["samples_valid"].endswith("samples_valid.npy")
+
+
+def test_bulk_two_workers_skip_and_failure(cuda, tmp_path):
+    """naja sample bulk (src/engine/job_bulk.cpp:115-267): two worker threads
+    on GPU 0 share three models; a job's samples are those `sample run`
+    gives for the same model directory and GPU; --skip-existing with
+    --resume-from reruns nothing; a model whose start is infeasible fails on
+    its own and fails the run."""
+    for k, name in enumerate(("B1", "B2", "B3")):
+        _model_dir(tmp_path, name, seed=10 + k)
+    root = tmp_path / "models"
+    lst = tmp_path / "list.txt"
+    lst.write_text("B1\nB2\nB3\n")
+    flags = ["--n-chains", 2, "--n-samples", 60, "--backmap", "--write-npy", "--bounds-policy", "filter",
+             "--resync-interval", 256, "--thinning", 3]
+    out = tmp_path / "out"
+    r = _run("sample", "bulk", "--models-root", root, "--model-list", lst, "--out-root", out, "--name", "RUN",
+             "--gpus", "0,0", *flags)
+    assert r.returncode == 0, r.stderr + r.stdout
+    assert "bulk sampling :: 3 jobs across 2 gpu(s)" in r.stdout and "completed : 3 / 3" in r.stdout
+    run = next(out.iterdir())
+    rows = [line.split(",") for line in (run / "bulk_summary.csv").read_text().splitlines()]
+    assert rows[0] == ["model", "status", "elapsed_s", "device_id", "message", "output_dir", "inherited_from_base"]
+    assert sorted(r_[0] for r_ in rows[1:]) == ["B1", "B2", "B3"]
+    assert all(r_[1] == "OK" and r_[3] == "0" for r_ in rows[1:])
+    for name in ("B1", "B2", "B3"):
+        jobs = list((run / name).iterdir())
+        assert len(jobs) == 1 and jobs[0].name.startswith(f"{name}_") and jobs[0].name.endswith("_001")
+        V_ = np.load(jobs[0] / "samples.npy")
+        assert V_.shape == (120, 130)
+        for f in ("profile.json", "config_used.txt", "valid_mask.npy", "valid_fraction.txt", "bounds_report.json"):
+            assert (jobs[0] / f).stat().st_size > 0
+    # the same job through `sample run` (same model directory string, same GPU): same seed, same samples
+    single = tmp_path / "single"
+    r = _run("sample", "run", "--model-dir", root / "B2", "--out-root", single, "--gpu", 0, *flags)
+    assert r.returncode == 0, r.stderr + r.stdout
+    assert np.array_equal(np.load(next(single.iterdir()) / "samples.npy"),
+                          np.load(next((run / "B2").iterdir()) / "samples.npy"))
+    # resume: every model is complete, nothing runs again
+    r = _run("sample", "bulk", "--models-root", root, "--model-list", lst, "--resume-from", run, "--name", "RUN",
+             "--gpus", "0", "--skip-existing", *flags)
+    assert r.returncode == 0, r.stderr + r.stdout
+    assert r.stdout.count("-> SKIP") == 3 and (run / "run_manifest_resume.json").exists()
+    assert all(len(list((run / n).iterdir())) == 1 for n in ("B1", "B2", "B3"))
+    # an infeasible start fails that job only
+    _write(root / "B3" / "rounding" / "B3_rounding_start.csv", np.full((40, 1), 1e6))
+    out2 = tmp_path / "out2"
+    r = _run("sample", "bulk", "--models-root", root, "--model-list", lst, "--out-root", out2, "--name", "RUN",
+             "--gpus", "0", *flags)
+    assert r.returncode == 1 and "bulk sampling failed" in r.stderr
+    rows = {r_.split(",")[0]: r_.split(",") for r_ in (next(out2.iterdir()) / "bulk_summary.csv").read_text().splitlines()[1:]}
+    assert rows["B1"][1] == "OK" and rows["B2"][1] == "OK" and rows["B3"][1] == "FAIL"
+    assert "infeasible start point" in rows["B3"][4]
 
 
 def _schedule(path, d, seed):
