@@ -196,6 +196,27 @@ def _backmap_error(torch, Tm, shift, samples_dev, V_dev, mode):
             "note": "relative error over |v| > 1e-3 max|v|; normalised = |err| / (|T||y| + |shift|)"}
 
 
+def _dgemm_backmap_ms(torch, T_dev, sh_dev, Z):
+    """The reference's backmap (cuBLAS DGEMM V = T Y, then + shift per
+    column; src/gpu/backmap.cu:20-48) on the same samples, FP64 operands
+    prepared untimed; mean of three after one warm-up."""
+    Zd = Z.double()
+    Td = T_dev.double()
+    out = torch.empty((Z.shape[0], Td.shape[0]), dtype=torch.float64, device=Z.device)
+    ms = []
+    for k in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(Zd, Td.T, out=out)
+        out.add_(sh_dev.double())
+        e1.record()
+        torch.cuda.synchronize()
+        if k:
+            ms.append(e0.elapsed_time(e1))
+    del Zd, Td, out
+    return statistics.mean(ms)
+
+
 def _backmap_roofline(W, ms, mode):
     flops = 2.0 * W.n * W.d * W.nspc * W.nchains
     p = ROOT / "MEASURED_PEAKS.json"
@@ -240,7 +261,8 @@ def _compact(line):
     bm = line.get("backmap")
     if bm:
         out["backmap"] = {"mode": bm["mode"], "ms": _r(bm["ms"]), "max_rel": _r(bm["error_vs_fp64"]["max_rel"], 3),
-                          "tflops": _r(bm["roofline"]["achieved"], 3)}
+                          "tflops": _r(bm["roofline"]["achieved"], 3), "frac": _r(bm["roofline"].get("frac", 0.0), 3),
+                          "y_map_ms": _r(bm.get("y_map_ms", 0.0), 3), "dgemm_ms": _r(bm.get("cublas_dgemm_ms"), 3)}
     if "e2e" in line:
         out["e2e"] = {k: _r(v, 5) for k, v in line["e2e"].items() if k != "timing"}
     if "cpu_baseline" in line:
@@ -372,11 +394,13 @@ def _ours(a, rank, world):
         P.run(x0, W.nspc, W.thin, W.nchains, out=zbuf, seed=seed, pair_prob=W.pair,
               resync_interval=a.resync, precision=a.precision, sparse=a.sparse, tpb=a.tpb)
         e_mid = torch.cuda.Event(enable_timing=True)
+        e_ymap = torch.cuda.Event(enable_timing=True)
         e_mid.record()
         if rounded:
             nb.backmap(M_dev, c_dev, zbuf, mode="fp64", out=samples)  # y = M z + c for the metric
+        e_ymap.record()
         nb.backmap(T_dev, sh_dev, zbuf, mode=a.backmap_mode, out=V)  # v = T' z + shift'
-        return e_mid
+        return e_mid, e_ymap
 
     for _ in range(a.warmup):
         job()
@@ -402,8 +426,9 @@ def _ours(a, rank, world):
     P.check()
     total_ms = g0.elapsed_time(g1)
     job_ms = [ev[k][0].elapsed_time(ev[k][1]) for k in range(a.steps)]
-    chr_ms = [ev[k][0].elapsed_time(mids[k]) for k in range(a.steps)]
-    bm_ms = [mids[k].elapsed_time(ev[k][1]) for k in range(a.steps)]
+    chr_ms = [ev[k][0].elapsed_time(mids[k][0]) for k in range(a.steps)]
+    ymap_ms = [mids[k][0].elapsed_time(mids[k][1]) for k in range(a.steps)]
+    bm_ms = [mids[k][1].elapsed_time(ev[k][1]) for k in range(a.steps)]
     # metric on the last job's samples
     ess, rhat = nv.ess_rhat(samples, W.nchains, layout=1)
     per_dim, total_ms = reduce_over_ranks(ess.sum(axis=1), total_ms, world, dev)
@@ -412,6 +437,7 @@ def _ours(a, rank, world):
     value = min_ess / (ms_per_step / 1e3)  # min-ESS already sums every rank's chains
     gate = _gate(torch, W, samples, ess, rhat)
     bm_err = _backmap_error(torch, Tp, shp, zbuf, V, a.backmap_mode)
+    dgemm_ms = _dgemm_backmap_ms(torch, T_dev, sh_dev, zbuf) if rank == 0 else None
     ref_sem = nv.summary(*nv.ess_rhat(samples, W.nchains, layout=0))
     peak, peak_kind = _peaks()
     choice = P.kernel_choice(W.nspc, W.thin, W.nchains, pair_prob=W.pair, resync_interval=a.resync,
@@ -438,14 +464,18 @@ def _ours(a, rank, world):
         "job_ms": _stats(job_ms), "chr_ms": _stats(chr_ms),
         "gate": gate,
         "backmap": {"mode": a.backmap_mode, "ms": statistics.mean(bm_ms), "error_vs_fp64": bm_err,
-                    "roofline": _backmap_roofline(W, statistics.mean(bm_ms), a.backmap_mode)},
+                    "roofline": _backmap_roofline(W, statistics.mean(bm_ms), a.backmap_mode),
+                    # y = M z + c of the rounded job (FP64 SIMT, for the metric), timed apart
+                    "y_map_ms": statistics.mean(ymap_ms),
+                    # the reference's backmap_into (src/gpu/backmap.cu:20-48): cuBLAS DGEMM + shift
+                    "cublas_dgemm_ms": dgemm_ms},
         "reference_semantics_validate": {k: ref_sem[k] for k in ("status", "ess", "rhat")},
         # per step: the CHR kernel, the y map (one FP64 kernel) when rounded, then the backmap
         # (one FP64 kernel, or operand split x2 + tcgen05 GEMM)
         "gpu_launches": a.steps * (1 + (1 if rounded else 0) + (1 if a.backmap_mode == "fp64" else 3)),
     }
     line["clocks"] = clk.summary()
-    detail = {"job_ms": job_ms, "chr_ms": chr_ms, "backmap_ms": bm_ms}
+    detail = {"job_ms": job_ms, "chr_ms": chr_ms, "backmap_ms": bm_ms, "y_map_ms": ymap_ms}
     if rank == 0 and rounded:
         line["plain"] = _plain_figure(a, W, torch, dev)
     if rank == 0 and a.fp64_figure:
@@ -726,6 +756,21 @@ def _precision_study(a):
         bm[mode] = {"max_rel": float(rel.max()), "rms_rel": float(rel.pow(2).mean().sqrt()), "ms_200k": ms,
                     "tflops": 2.0 * 7000 * 1500 * 200000 / (ms / 1e3) / 1e12}
         del V, Vb
+    Yd, Td = Ybig.double(), T.double()
+    Vd = torch.empty((200000, 7000), dtype=torch.float64, device=dev)
+    ms = []
+    for k in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(Yd, Td.T, out=Vd)  # the reference's backmap_into: cuBLAS DGEMM, then + shift
+        Vd.add_(sh.double())
+        e1.record()
+        torch.cuda.synchronize()
+        if k:
+            ms.append(e0.elapsed_time(e1))
+    bm["cublas_dgemm"] = {"max_rel": 0.0, "rms_rel": 0.0, "ms_200k": statistics.mean(ms),
+                          "tflops": 2.0 * 7000 * 1500 * 200000 / (statistics.mean(ms) / 1e3) / 1e12}
+    del Yd, Td, Vd
     P.close()
     return {"workload": "genome-shaped n=7000 d=1500 m=14000, 8 chains x 200 samples, thinning 256, pair 0.3",
             "chr": rows, "backmap": bm}

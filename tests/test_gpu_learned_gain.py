@@ -9,9 +9,12 @@ axes mixes slowly in such an elongated, rotated box.  The network
 diagonal-plus-rank-5 factors of plain-CHR sample covariances of 48 training
 variants, then predicts the rounding of 8 held-out variants.  At the same
 number of CHR steps, learned-rounded CHR must give at least twice the
-min-ESS of plain CHR (median over held-out variants), every sample must
-satisfy the original constraints, and the network must predict the
-held-out targets better than their training mean.
+min-ESS of plain CHR and at least 1.5 times that of CHR rounded by the
+reference's Dikin preconditioner (median over held-out variants; the
+rounded polytopes have the same rows and columns, so a step costs the same
+and the min-ESS ratio is the min-ESS/s ratio), every sample must satisfy
+the original constraints, and the network must predict the held-out
+targets better than their training mean.
 """
 import numpy as np
 import pytest
@@ -44,7 +47,7 @@ def _min_ess(y, nchains):
     return float(V.chain_ess(ess).min())
 
 
-def test_learned_rounding_beats_plain(cuda):
+def test_learned_rounding_beats_plain_and_dikin(cuda):
     train, test = _family(48, 1), _family(8, 2)
     # targets: factors of plain-CHR sample covariances
     T = []
@@ -62,7 +65,7 @@ def test_learned_rounding_beats_plain(cuda):
     Ft = np.array([f for f, _, _ in test], np.float32)
     pred = net.predict(Ft).cpu().numpy() * sd + mu
 
-    gains, err_net, err_mean = [], [], []
+    gains, gains_dikin, err_net, err_mean = [], [], [], []
     for j, (_, A, b) in enumerate(test):
         P = Polytope(A, b)
         Y0 = P.run(np.zeros(D), 400, 8, 8, seed=100 + j, out_dtype="f64")
@@ -72,12 +75,18 @@ def test_learned_rounding_beats_plain(cuda):
         Y1 = r.to_y(Z)
         assert (Y1 @ A.T - b).max() <= 1e-6 * np.abs(b).max()
         gains.append(_min_ess(Y1, 8) / _min_ess(Y0, 8))
+        rd = rounding.dikin(A, b, np.zeros(D))
+        Y2 = rd.to_y(Polytope(rd.A, rd.b).run(rd.z0, 400, 8, 8, seed=100 + j, out_dtype="f64"))
+        assert (Y2 @ A.T - b).max() <= 1e-6 * np.abs(b).max()
+        gains_dikin.append(_min_ess(Y1, 8) / _min_ess(Y2, 8))
         # how well the held-out rounding is predicted, against the long-run target
         Yl = P.run(np.zeros(D), 1500, 40, 16, seed=200 + j, out_dtype="f64")
         tgt = pack(*factor_target(np.cov(Yl.T), RANK))
         err_net.append(np.mean(((pred[j] - tgt) / sd) ** 2))
         err_mean.append(np.mean(((mu - tgt) / sd) ** 2))
     print(f"learned / plain min-ESS per held-out variant: {np.round(gains, 2).tolist()}; "
+          f"learned / Dikin: {np.round(gains_dikin, 2).tolist()}; "
           f"prediction MSE {np.mean(err_net):.3f} vs mean predictor {np.mean(err_mean):.3f}")
     assert np.median(gains) >= 2.0, gains
+    assert np.median(gains_dikin) >= 1.5, gains_dikin
     assert np.mean(err_net) < np.mean(err_mean), (np.mean(err_net), np.mean(err_mean))
