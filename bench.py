@@ -56,6 +56,13 @@ sys.path.insert(0, str(ROOT))
 METRIC = "min-ESS/sec at split-R-hat<1.01, learned-rounded vs plain CHR, 1 B200"
 UNIT = "min-ESS/s"
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes (read + write) of one launch of the headline step kernel,
+# chr_kernel<float, 512, 8> on the rounded genome-shaped job (n 2600, d 700,
+# 16 chains x 12,500 samples, thinning 116, pair 0.3, resync 2048, FP32,
+# Philox seed 0): one ncu capture of the full-size launch with
+# dram__bytes_read.sum 84.34 MB + dram__bytes_write.sum 549.55 MB.  Reported
+# as roofline.traffic only for that exact workload.
+HEADLINE_TRAFFIC_BYTES = 84.34e6 + 549.55e6
 
 
 def _peaks():
@@ -194,6 +201,14 @@ def _backmap_error(torch, Tm, shift, samples_dev, V_dev, mode):
             "rms_rel": float(torch.sqrt((rel ** 2).mean())),
             "max_normalised": float((err / scale.clamp(min=1e-300)).max()),
             "note": "relative error over |v| > 1e-3 max|v|; normalised = |err| / (|T||y| + |shift|)"}
+
+
+def _headline_traffic(a, W, choice):
+    """The captured DRAM bytes of the headline launch, where this run is that
+    launch's workload (else None: traffic was not captured for it)."""
+    same = (W.n, W.d, W.nchains, W.nspc, W.thin, W.pair, a.resync, a.precision, a.seed, a.rounding) == \
+        (2600, 700, 16, 12500, 116, 0.3, 2048, "fp32", 0, "dikin_full")
+    return HEADLINE_TRAFFIC_BYTES if same and choice["kernel"] != "columns" and choice["threads"] == 512 else None
 
 
 def _dgemm_backmap_ms(torch, T_dev, sh_dev, Z):
@@ -451,7 +466,7 @@ def _ours(a, rank, world):
         "dtype": "f32" if a.precision == "fp32" else "f64", "data": "synthetic (seeded genome-shaped generator)",
         "config": W.config(a),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_source": peak_kind,
+                     "traffic": _headline_traffic(a, W, choice), "peak_source": peak_kind,
                      "kernel": "chr_sparse_kernel" if choice["kernel"] == "columns" else "chr_kernel",
                      "kernel_threads": choice["threads"], "kernel_ms": chr_mean,
                      "bytes_per_chr_step": W.bytes_per_step,
