@@ -203,6 +203,16 @@ def _backmap_error(torch, Tm, shift, samples_dev, V_dev, mode):
             "note": "relative error over |v| > 1e-3 max|v|; normalised = |err| / (|T||y| + |shift|)"}
 
 
+def _chr_launches(W, a, choice):
+    """Kernels one CHR run launches: a dense run with a recompute interval K
+    shorter than the run and m d >= 2^19 runs in segments of K steps, each a
+    slack-recompute kernel and a step kernel."""
+    total = W.nspc * W.thin
+    if choice["kernel"] == "dense" and 0 < a.resync < total and W.m * W.d >= (1 << 19):
+        return 2 * (-(-total // a.resync))
+    return 1
+
+
 def _headline_traffic(a, W, choice):
     """The captured DRAM bytes of the headline launch, where this run is that
     launch's workload (else None: traffic was not captured for it)."""
@@ -485,9 +495,12 @@ def _ours(a, rank, world):
                     # the reference's backmap_into (src/gpu/backmap.cu:20-48): cuBLAS DGEMM + shift
                     "cublas_dgemm_ms": dgemm_ms},
         "reference_semantics_validate": {k: ref_sem[k] for k in ("status", "ess", "rhat")},
-        # per step: the CHR kernel, the y map (one FP64 kernel) when rounded, then the backmap
-        # (one FP64 kernel, or operand split x2 + tcgen05 GEMM)
-        "gpu_launches": a.steps * (1 + (1 if rounded else 0) + (1 if a.backmap_mode == "fp64" else 3)),
+        # per step: the CHR run (one step kernel, or per recompute interval one
+        # slack-recompute kernel and one step kernel), the y map (one FP64
+        # kernel) when rounded, then the backmap (one FP64 kernel, or operand
+        # split x2 + tcgen05 GEMM)
+        "gpu_launches": a.steps * (_chr_launches(W, a, choice) + (1 if rounded else 0)
+                                   + (1 if a.backmap_mode == "fp64" else 3)),
     }
     line["clocks"] = clk.summary()
     detail = {"job_ms": job_ms, "chr_ms": chr_ms, "backmap_ms": bm_ms, "y_map_ms": ymap_ms}

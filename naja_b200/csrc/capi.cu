@@ -644,8 +644,13 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
   a.wait_cycles = p->wait_cycles;
   a.slack_final = dsf;
 
-  st = use_sparse ? chr_sparse_launch(p->precision, a, spa, p->nchains, cfg, stream)
-                  : chr_launch(p->precision, a, p->nchains, cfg, stream);
+  const long long total_steps = static_cast<long long>(p->nspc) * p->thinning;
+  if (use_sparse)
+    st = chr_sparse_launch(p->precision, a, spa, p->nchains, cfg, stream);
+  else if (chr_use_segments(P->m, d, p->resync_interval, total_steps, cfg.cluster, p->wait_cycles != nullptr))
+    st = chr_run_segmented(p->precision, a, p->nchains, cfg, stream, nullptr);
+  else
+    st = chr_launch(p->precision, a, p->nchains, cfg, stream);
   if (st) {
     cudaError_t e = cudaGetLastError();
     return fail(st, std::string("CoordinateHitAndRun: launch failed: ") + cudaGetErrorString(e));

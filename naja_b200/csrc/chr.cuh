@@ -46,6 +46,15 @@ struct ChrArgs {
   // Nullable: receives each chain's slack b - A x after its last step
   // (nchains x m values of the tier's type, chain-major).
   void* slack_final;
+  // Step range of this launch within the chains' run: steps t_first ..
+  // t_first + steps - 1 (steps 0: nspc * thinning steps from t_first 0).
+  // Saved samples (every thinning-th global step, output row = global step /
+  // thinning), Philox steps (step_offset + global step) and the resync
+  // schedule (global multiples of resync) follow the global step index.
+  long long t_first, steps;
+  // Nullable: each chain's slack at step t_first (the tier's type,
+  // chain-major, nchains x m), read instead of the initial FP64 recompute.
+  const void* slack_in;
 };
 
 struct ChrLaunchConfig {
@@ -101,6 +110,33 @@ int chr_plan(int precision, int m, int d, int lda, int tpb, int max_slots, int n
 
 // Launches nchains independent chains (one CTA each) on `stream`.
 int chr_launch(int precision, const ChrArgs& args, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+
+// Runs the same chains as one chr_launch with args.resync = K > 0, as
+// segments of K steps: before each segment one kernel over the whole GPU
+// recomputes every chain's slack b - A64 x in FP64 (each row's fma chain
+// over the columns in order, as the step kernel's recompute), and the
+// segment's step kernel starts from it (slack_in) with no recompute of its
+// own.  Samples, final positions, final slack and RNG streams are those of
+// the single launch, bit for bit; the recompute, which the step kernel
+// does on the chain's one SM, reads A64 on every SM instead.  Returns the
+// number of kernel launches through `launches` (nullable).
+int chr_run_segmented(int precision, const ChrArgs& args, int nchains, const ChrLaunchConfig& cfg,
+                      cudaStream_t stream, long long* launches);
+
+// Steps of one launch (host side of the kernels' launch_steps).
+inline long long launch_steps_host(const ChrArgs& a) {
+  return a.steps > 0 ? a.steps : static_cast<long long>(a.nspc) * a.thinning;
+}
+
+// True where chr_run_segmented pays for its per-segment launches: a dense
+// single-CTA run with a recompute interval shorter than the run and an A64
+// large enough (m d >= kSegmentMinCells) that reading it from one SM costs
+// more than a segment boundary.
+constexpr long long kSegmentMinCells = 1LL << 19;
+inline bool chr_use_segments(long long m, long long d, int resync, long long total_steps, int cluster,
+                             bool instrumented) {
+  return resync > 0 && total_steps > resync && cluster <= 1 && !instrumented && m * d >= kSegmentMinCells;
+}
 
 // Records the first `count` uniforms of curand_init(seed, chain_base + c, 0)
 // MRG32k3a states, c < nchains, into tape[c * count + i] (device memory).

@@ -40,6 +40,80 @@ __global__ void mrg_init_kernel(unsigned long long seed, int chain_base, int nch
   if (c < nchains) curand_init(seed, static_cast<unsigned long long>(chain_base + c), 0ull, &st[c]);
 }
 
+// slack[c][r] = b[r] - sum_j A64[r][j] x_c[j] for every chain c, in FP64
+// with each row's fma chain over j in order from 0.0 (the step kernel's
+// recompute), rounded to the tier's type.  One thread per row for kSlackCG
+// chains (they share every load of A64), the CTA's chains' x in shared
+// memory (XS) or read from global memory (every lane the same address).
+// The loop is latency-bound, so each thread loads kSlackJB values of its row
+// before their fmas: kSlackJB loads in flight per thread.
+constexpr int kSlackCG = 2;
+constexpr int kSlackJB = 16;
+template <class Real, bool XS>
+__global__ void __launch_bounds__(128) slack_recompute_kernel(const double* __restrict__ A64, int lda,
+                                                              const double* __restrict__ b, int m, int d,
+                                                              const double* __restrict__ X, int ldx, int nchains,
+                                                              Real* __restrict__ slack) {
+  extern __shared__ double xsh[];  // XS: kSlackCG x d
+  const int c0 = blockIdx.y * kSlackCG;
+  const int nc = nchains - c0 < kSlackCG ? nchains - c0 : kSlackCG;
+  const double* xv = X + static_cast<size_t>(c0) * ldx;
+  int ldv = ldx;
+  if constexpr (XS) {
+    for (int i = threadIdx.x; i < nc * d; i += blockDim.x) {
+      const int c = i / d, j = i - c * d;
+      xsh[c * d + j] = xv[static_cast<size_t>(c) * ldx + j];
+    }
+    __syncthreads();
+    xv = xsh;
+    ldv = d;
+  }
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= m) return;
+  double acc[kSlackCG];
+#pragma unroll
+  for (int c = 0; c < kSlackCG; ++c) acc[c] = 0.0;
+  const double* Ar = A64 + r;
+  // a CTA with fewer than kSlackCG chains repeats its last one (not stored),
+  // which keeps the loop free of branches
+  const double* xc[kSlackCG];
+#pragma unroll
+  for (int c = 0; c < kSlackCG; ++c) xc[c] = xv + static_cast<size_t>(c < nc ? c : nc - 1) * ldv;
+  int j = 0;
+  for (; j + kSlackJB <= d; j += kSlackJB) {
+    double av[kSlackJB];
+#pragma unroll
+    for (int u = 0; u < kSlackJB; ++u) av[u] = __ldg(Ar + static_cast<size_t>(j + u) * lda);
+#pragma unroll
+    for (int u = 0; u < kSlackJB; ++u)
+#pragma unroll
+      for (int c = 0; c < kSlackCG; ++c) acc[c] = __fma_rn(av[u], xc[c][j + u], acc[c]);
+  }
+  for (; j < d; ++j) {
+    const double av = __ldg(Ar + static_cast<size_t>(j) * lda);
+#pragma unroll
+    for (int c = 0; c < kSlackCG; ++c) acc[c] = __fma_rn(av, xc[c][j], acc[c]);
+  }
+#pragma unroll
+  for (int c = 0; c < kSlackCG; ++c)
+    if (c < nc) slack[static_cast<size_t>(c0 + c) * m + r] = Tier<Real>::from64(__dsub_rn(b[r], acc[c]));
+}
+
+// Launches slack_recompute_kernel for every chain of x (leading dimension ldx).
+template <class Real>
+int slack_recompute(const ChrArgs& a, const double* x, int ldx, int nchains, Real* slack, cudaStream_t stream) {
+  const dim3 grid((a.m + 127) / 128, (nchains + kSlackCG - 1) / kSlackCG);
+  const size_t xs_bytes = static_cast<size_t>(kSlackCG) * a.d * sizeof(double);
+  if (xs_bytes <= 48 * 1024) {
+    slack_recompute_kernel<Real, true><<<grid, 128, xs_bytes, stream>>>(a.A64, a.lda, a.b, a.m, a.d, x, ldx,
+                                                                         nchains, slack);
+  } else {
+    slack_recompute_kernel<Real, false><<<grid, 128, 0, stream>>>(a.A64, a.lda, a.b, a.m, a.d, x, ldx, nchains,
+                                                                   slack);
+  }
+  return cudaGetLastError() == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
+}
+
 // Largest chunks-per-warp capacity instantiated for a thread count (the
 // slack of R chunks takes R * kStandaloneV registers per thread).
 int max_chunks_for(int threads) { return threads <= 512 ? 16 : 8; }
@@ -159,6 +233,71 @@ int chr_launch(int precision, const ChrArgs& args, int nchains, const ChrLaunchC
     case 992: return f64 ? chr_launch_double_992(args, nchains, cfg, stream) : chr_launch_float_992(args, nchains, cfg, stream);
     default: return NAJA_ERR_UNSUPPORTED;
   }
+}
+
+int chr_run_segmented(int precision, const ChrArgs& a0, int nchains, const ChrLaunchConfig& cfg,
+                      cudaStream_t stream, long long* launches) {
+  if (launches) *launches = 0;
+  if (nchains <= 0) return NAJA_OK;
+  const long long K = a0.resync;
+  const long long total = launch_steps_host(a0);
+  if (K <= 0 || a0.t_first != 0 || a0.slack_in) return NAJA_ERR_INVALID_ARGUMENT;
+  const long long nseg = (total + K - 1) / K;
+  const int d = a0.d, m = a0.m;
+  const size_t elt = precision == NAJA_PREC_FP64 ? sizeof(double) : sizeof(float);
+  const size_t x_bytes = static_cast<size_t>(nchains) * d * sizeof(double);
+  const size_t s_bytes = static_cast<size_t>(nchains) * m * elt;
+  const bool own_states = a0.rng != 0 && !a0.rng_state;
+  void *xb = nullptr, *sb = nullptr, *rs = nullptr;
+  auto release = [&]() {
+    if (xb) cudaFreeAsync(xb, stream);
+    if (sb) cudaFreeAsync(sb, stream);
+    if (rs) cudaFreeAsync(rs, stream);
+  };
+  cudaError_t e = cudaMallocAsync(&xb, 2 * x_bytes, stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(&sb, s_bytes, stream);
+  if (e == cudaSuccess && own_states) e = cudaMallocAsync(&rs, nchains * sizeof(curandStateMRG32k3a), stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    release();
+    return NAJA_ERR_NO_MEMORY;
+  }
+  double* xs[2] = {static_cast<double*>(xb), static_cast<double*>(xb) + static_cast<size_t>(nchains) * d};
+  // positions travel between segments chain-major with leading dimension d
+  e = cudaMemcpy2DAsync(xs[0], d * sizeof(double), a0.X0, static_cast<size_t>(a0.ldx) * sizeof(double),
+                        d * sizeof(double), nchains, cudaMemcpyDeviceToDevice, stream);
+  int st = e == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
+  long long n_launch = 0;
+  if (!st && own_states) {
+    st = mrg_init_states(a0.seed, a0.chain_base, nchains, rs, stream);
+    ++n_launch;
+  }
+  for (long long s = 0; s < nseg && !st; ++s) {
+    const double* xin = xs[s % 2];
+    st = precision == NAJA_PREC_FP64 ? slack_recompute(a0, xin, d, nchains, static_cast<double*>(sb), stream)
+                                     : slack_recompute(a0, xin, d, nchains, static_cast<float*>(sb), stream);
+    if (st) break;
+    ChrArgs a = a0;
+    a.X0 = xin;
+    a.ldx = d;
+    a.X_final = xs[(s + 1) % 2];
+    a.t_first = s * K;
+    a.steps = total - s * K < K ? total - s * K : K;
+    a.slack_in = sb;
+    a.resync = 0;  // this segment's recompute is the one just made
+    a.slack_final = s + 1 == nseg ? a0.slack_final : nullptr;
+    if (own_states) a.rng_state = rs;
+    st = chr_launch(precision, a, nchains, cfg, stream);
+    n_launch += 2;
+  }
+  if (!st && a0.X_final) {
+    e = cudaMemcpy2DAsync(a0.X_final, static_cast<size_t>(a0.ldx) * sizeof(double), xs[nseg % 2],
+                          d * sizeof(double), d * sizeof(double), nchains, cudaMemcpyDeviceToDevice, stream);
+    if (e != cudaSuccess) st = NAJA_ERR_CUDA;
+  }
+  release();
+  if (launches) *launches = n_launch;
+  return st;
 }
 
 int mrg_tape(unsigned long long seed, int chain_base, int nchains, long count, double* tape, cudaStream_t stream) {

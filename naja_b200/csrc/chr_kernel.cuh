@@ -377,6 +377,11 @@ struct Tier<double> {
 };
 
 
+// Steps of one launch (ChrArgs::t_first, ChrArgs::steps).
+__device__ __forceinline__ long long launch_steps(const ChrArgs& a) {
+  return a.steps > 0 ? a.steps : static_cast<long long>(a.nspc) * a.thinning;
+}
+
 // ------------------------------------------------------------------ producer
 // One thread: draws each step's direction ahead of the consumers, claims one
 // ring slot per staged column (two for a pair step, one metadata-only slot
@@ -394,7 +399,7 @@ __device__ __noinline__ void run_producer(const ChrArgs& a, Src& src, const Layo
   const Real* A = Tier<Real>::A(a);
   const uint32_t col_bytes = static_cast<uint32_t>(align_up(static_cast<size_t>(a.m) * sizeof(Real), 16));
   const int S = L.slots;
-  const long long total = static_cast<long long>(a.nspc) * a.thinning;
+  const long long total = launch_steps(a);
   // Slots are claimed round-robin.  `slot` is the next one, `round` how many
   // times the ring has wrapped: a slot's use number is the round it is
   // claimed in, its fill waits for the empty-barrier phase of round - 1.
@@ -408,7 +413,7 @@ __device__ __noinline__ void run_producer(const ChrArgs& a, Src& src, const Layo
   const unsigned long long p_start = clock64();
   for (long long t = 0; t < total; ++t) {
     if (*abort_flag) break;
-    src.begin_step(static_cast<uint64_t>(a.step_offset + t));
+    src.begin_step(static_cast<uint64_t>(a.step_offset + a.t_first + t));
     if (!draw_direction(src, a, dir, ks_idx, ks_coef)) {
       set_error(a.err, kDevBadPair, dir.ei, dir.ej, static_cast<int>(t));
       *abort_flag = 1;
@@ -713,15 +718,36 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
           }
         });
   };
-  recompute();
+  if (a.slack_in) {
+    // the slack at step t_first, computed outside the kernel
+    const Real* si = static_cast<const Real*>(a.slack_in) + static_cast<size_t>(chain_local) * m;
+    for_chunks(
+        [&](int k, int base) {
+          Real sv[V];
+#pragma unroll
+          for (int v = 0; v < V; ++v) sv[v] = si[base + v];
+          slack_put(k, base, sv);
+        },
+        [&](int base) {
+#pragma unroll
+          for (int v = 0; v < V; ++v)
+            if (base + v < m) slack_tail(base + v) = si[base + v];
+        });
+  } else {
+    recompute();
+  }
 
-  const long long total = static_cast<long long>(a.nspc) * a.thinning;
+  const long long total = launch_steps(a);
   // Ring position (mirrors the producer), phase parity of the slot's fill,
-  // and step counters that replace t % thinning, t / thinning, t % resync.
+  // and step counters that replace the global step's remainders modulo
+  // thinning and resync; out_row is the next saved sample's row.
   int slot = 0;
   uint32_t parity = 0;
-  int thin_ctr = 0, resync_ctr = 0, rbuf = 0;
-  size_t out_row = static_cast<size_t>(gchain);
+  int thin_ctr = static_cast<int>(a.t_first % a.thinning);
+  int resync_ctr = a.resync > 0 ? static_cast<int>(a.t_first % a.resync) : 0;
+  int rbuf = 0;
+  size_t out_row = static_cast<size_t>(gchain) +
+                   static_cast<size_t>((a.t_first + a.thinning - 1) / a.thinning) * a.out_nchains;
   unsigned long long w_full = 0;
   const unsigned long long c_start = TIMING ? clock64() : 0ull;
   Real ae_prev[FUSED ? R * V : 1];   // step t-1's column values of this lane's rows
@@ -773,7 +799,8 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
     }
     // Uniform across every consumer warp (a named barrier follows), whatever `ok` is.
     if (a.resync > 0) {
-      if (resync_ctr == 0) {
+      // (the launch's first step starts from the slack computed before the loop)
+      if (resync_ctr == 0 && t != 0) {
         named_bar_sync(2, NT);  // every owner's x update of the previous step is visible
         recompute();
         pending = false;        // the recompute already holds step t-1's move

@@ -209,7 +209,13 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
     }
     if (tid == 0) slack[m] = Real(0);
   };
-  recompute();
+  if (a.slack_in) {
+    const Real* si = static_cast<const Real*>(a.slack_in) + static_cast<size_t>(chain_local) * m;
+    for (int r = tid; r < m; r += NT) slack[r] = si[r];
+    if (tid == 0) slack[m] = Real(0);
+  } else {
+    recompute();
+  }
   consumers_sync<NW>(1);
 
   // Cross-warp max / min: lane 0 of each warp posts, one barrier, every
@@ -240,11 +246,15 @@ __device__ void run_sparse_consumers(const ChrArgs& a, const SpArgs& sp, const L
     }
   };
 
-  const long long total = static_cast<long long>(a.nspc) * a.thinning;
+  // global step counters as in the dense kernel (ChrArgs::t_first)
+  const long long total = launch_steps(a);
   int slot = 0;
   uint32_t parity = 0;
-  int thin_ctr = 0, resync_ctr = 0, abuf = 0;
-  size_t out_row = static_cast<size_t>(gchain);
+  int thin_ctr = static_cast<int>(a.t_first % a.thinning);
+  int resync_ctr = a.resync > 0 ? static_cast<int>(a.t_first % a.resync) : 0;
+  int abuf = 0;
+  size_t out_row = static_cast<size_t>(gchain) +
+                   static_cast<size_t>((a.t_first + a.thinning - 1) / a.thinning) * a.out_nchains;
   unsigned long long w_full = 0;
   const unsigned long long c_start = clock64();
   for (long long t = 0; t < total; ++t) {
