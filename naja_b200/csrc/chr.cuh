@@ -66,6 +66,8 @@ struct ChrLaunchConfig {
   int slice_lda;  // rows a CTA's column slot holds (cluster > 1), padded to 32
   int max_col;    // sparse-column kernel: entries of the longest compressed column
   int pair_scatter;  // sparse-column kernel: 1 = pair steps through a scratch column, 0 = by search
+  int uniform;       // dense single-CTA kernel: 1 = every warp runs `rows` chunks, the rows past m
+                     // repeating the last V rows (needs m % V == 0); 0 = chunks as rows allow
 };
 
 // Compressed columns of A for the sparse-column kernel, in the tier's

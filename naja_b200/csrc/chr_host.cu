@@ -114,9 +114,11 @@ int slack_recompute(const ChrArgs& a, const double* x, int ldx, int nchains, Rea
   return cudaGetLastError() == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
 }
 
-// Largest chunks-per-warp capacity instantiated for a thread count (the
-// slack of R chunks takes R * kStandaloneV registers per thread).
-int max_chunks_for(int threads) { return threads <= 512 ? 16 : 8; }
+// Largest chunks-per-warp capacity used for a thread count (the slack of R
+// chunks takes R * V registers per thread, V rows per lane and chunk).
+int max_chunks_for(int threads, int v) { return (threads <= 512 ? 32 : 16) / v; }
+// Largest chunk count of the uniform-chunk kernels (instantiated 1..8).
+constexpr int kMaxUniformChunks = 8;
 
 }  // namespace
 
@@ -138,11 +140,11 @@ int plan_single(int precision, int m, int d, int lda, int tpb, int max_slots, Ch
     while (threads < 512 && (m + threads - 1) / threads > 12) threads *= 2;
     if ((m + threads - 1) / threads > 16) threads = 992;
   }
-  const int chunk = 32 * kStandaloneV;
+  const int chunk = 32 * standalone_v(precision);
   const int chunks = (m + chunk - 1) / chunk, warps = threads / 32;
   int rows = 1;
   while (rows * warps < chunks) rows *= 2;
-  if (rows > max_chunks_for(threads)) return NAJA_ERR_UNSUPPORTED;
+  if (rows > max_chunks_for(threads, standalone_v(precision))) return NAJA_ERR_UNSUPPORTED;
   int slots = kMaxSlots;
   if (max_slots > 0 && max_slots < slots) slots = max_slots;
   Layout L = make_layout(d, lda, elt, threads, slots);
@@ -163,6 +165,14 @@ int plan_single(int precision, int m, int d, int lda, int tpb, int max_slots, Ch
   out->slice_lda = lda;
   out->max_col = 0;
   out->pair_scatter = 0;
+  out->uniform = 0;
+  // Uniform chunks: every warp runs the same R = ceil(chunks / warps)
+  // chunks as one straight-line row pass (rows past m repeat the last V).
+  const int v = standalone_v(precision), exact = (chunks + warps - 1) / warps;
+  if (m % v == 0 && m >= v && exact <= kMaxUniformChunks && exact <= max_chunks_for(threads, v)) {
+    out->uniform = 1;
+    out->rows = exact;
+  }
   return NAJA_OK;
 }
 
@@ -170,7 +180,7 @@ int plan_single(int precision, int m, int d, int lda, int tpb, int max_slots, Ch
 // per thread of the CTA's slice), the slot ring sized for the slice.
 int plan_cluster(int precision, int m, int d, int tpb, int max_slots, int cs, ChrLaunchConfig* out) {
   const int elt = precision == NAJA_PREC_FP64 ? 8 : 4;
-  const int chunk = 32 * kStandaloneV;
+  const int chunk = 32 * kClusterV;
   const int nc = (m + chunk - 1) / chunk;
   if (cs < 2 || cs > 8 || nc < cs) return NAJA_ERR_UNSUPPORTED;
   const int slice_chunks = (nc + cs - 1) / cs;
@@ -185,7 +195,7 @@ int plan_cluster(int precision, int m, int d, int tpb, int max_slots, int cs, Ch
   const int warps = threads / 32;
   int rows = 1;
   while (rows * warps < slice_chunks) rows *= 2;
-  if (rows > max_chunks_for(threads)) return NAJA_ERR_UNSUPPORTED;
+  if (rows > max_chunks_for(threads, kClusterV)) return NAJA_ERR_UNSUPPORTED;
   const int slda = (slice_rows + 31) / 32 * 32;
   int slots = kMaxSlots;
   if (max_slots > 0 && max_slots < slots) slots = max_slots;
@@ -204,6 +214,7 @@ int plan_cluster(int precision, int m, int d, int tpb, int max_slots, int cs, Ch
   out->slice_lda = slda;
   out->max_col = 0;
   out->pair_scatter = 0;
+  out->uniform = 0;
   return NAJA_OK;
 }
 }  // namespace

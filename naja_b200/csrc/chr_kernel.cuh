@@ -614,10 +614,18 @@ struct ClusterCtx {
 // with step t-1's column values kept in registers (R V per lane), so each
 // step makes one pass over its rows and releases its column slot right
 // after that pass.  The values are exactly those of the two-pass order.
+// UNI: every warp runs exactly R chunks with no test on the chunk count, so
+// a step's row pass is one straight-line block (its loads, divisions and
+// extremes can overlap across all R V rows of a lane).  Chunk k of a lane
+// covers rows min(base0 + k NW C, m - V) + v: past the last row the lanes
+// repeat the last V rows (m % V == 0 keeps that group aligned and whole),
+// whose ratios, slack and updates are bit for bit those of the rows they
+// repeat, so the extremes are unchanged; only the owner of a row writes it.
 template <class Real, int NT, int R, int V, bool SS = false, bool TIMING = true, bool MAYBE_DIRECT = true,
-          bool CL = false, bool FUSED = false>
+          bool CL = false, bool FUSED = false, bool UNI = false>
 __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* smem, int chain_local,
                               const ClusterCtx* cx = nullptr) {
+  static_assert(!UNI || (!SS && !CL), "uniform chunks keep the slack in registers, one CTA per chain");
   using T = Tier<Real>;
   using Acc = typename T::Acc;
   using UT = typename T::UType;
@@ -639,7 +647,7 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
   // partial chunk at k == my_full.
   const int n_full = m / C;
   const int my_full = n_full > warp ? (n_full - warp + NW - 1) / NW : 0;
-  const bool my_tail = (m % C) != 0 && (n_full % NW) == warp;
+  const bool my_tail = !UNI && (m % C) != 0 && (n_full % NW) == warp;
   const int base0 = warp * C + lane * V;
 
   for (int j = tid; j < d; j += NT) xs[j] = a.X0[static_cast<size_t>(chain_local) * a.ldx + j];
@@ -651,12 +659,17 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
   // owns it.
   const int tail_base = base0 + my_full * NW * C;
   auto for_chunks = [&](auto&& full_fn, auto&& tail_fn) {
+    if constexpr (UNI) {
 #pragma unroll
-    for (int k = 0; k < R; ++k) {
-      if (k >= my_full) break;
-      full_fn(k, base0 + k * NW * C);
+      for (int k = 0; k < R; ++k) full_fn(k, min(base0 + k * NW * C, m - V));
+    } else {
+#pragma unroll
+      for (int k = 0; k < R; ++k) {
+        if (k >= my_full) break;
+        full_fn(k, base0 + k * NW * C);
+      }
+      if (my_tail) tail_fn(tail_base);
     }
-    if (my_tail) tail_fn(tail_base);
   };
 
   Real sl_reg[SS ? 1 : R * V];
@@ -1039,6 +1052,7 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
     Real* so = static_cast<Real*>(a.slack_final) + static_cast<size_t>(chain_local) * m;
     for_chunks(
         [&](int k, int base) {
+          if (UNI && base0 + k * NW * C >= m) return;  // a repeat of rows another lane owns
           Real s[V];
           slack_get(k, base, s);
           if constexpr (FUSED) {
@@ -1070,15 +1084,21 @@ __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* 
   }
 }
 
-// Rows per lane per chunk of the single-model kernel: 8- (FP32) or 16-byte
-// (FP64) vector accesses, 64-row chunks; shorter chunks spread a model's rows
-// evenly over many warps, which bounds the latency of one step.
-constexpr int kStandaloneV = 2;
+// Rows per lane per chunk of the single-model kernel: 16-byte vector
+// accesses (FP32: 128-row chunks, four independent rows per lane between a
+// column load and the extremes; FP64: 64-row chunks, whose slack fits the
+// registers without spilling).
+template <class Real>
+constexpr int kStandaloneV = sizeof(Real) == 4 ? 4 : 2;
+inline int standalone_v(int precision) { return precision == NAJA_PREC_FP64 ? 2 : 4; }
+// A chain split over a cluster keeps 64-row chunks, so that small models
+// still give every CTA of the cluster rows.
+constexpr int kClusterV = 2;
 // The batched kernel (FP32 only) runs several chains per SM and is bound by
 // instruction issue, so it takes 16-byte accesses: 128-row chunks.
 constexpr int kBatchV = 4;
 
-template <class Real, int NT, int R>
+template <class Real, int NT, int R, bool UNI = false>
 __global__ void __launch_bounds__(NT + 32, 1)
     chr_kernel(const __grid_constant__ ChrArgs a, const __grid_constant__ Layout L) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -1100,8 +1120,8 @@ __global__ void __launch_bounds__(NT + 32, 1)
   }
   // fused update where step t-1's column values (R V per lane) fit in 64
   // bytes of registers; larger capacities keep the two-pass order
-  constexpr bool kFuse = R * kStandaloneV * sizeof(Real) <= 64;
-  run_consumers<Real, NT, R, kStandaloneV, false, true, true, false, kFuse>(a, L, smem, chain_local);
+  constexpr bool kFuse = R * kStandaloneV<Real> * sizeof(Real) <= 64;
+  run_consumers<Real, NT, R, kStandaloneV<Real>, false, true, true, false, kFuse, UNI>(a, L, smem, chain_local);
 }
 
 // One chain split over a thread-block cluster of `size` CTAs: CTA `rank`
@@ -1123,7 +1143,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
   __shared__ int xflag[2];
   const uint32_t rank = cluster_rank(), size = cluster_size();
   const int chain_local = static_cast<int>(blockIdx.x / size);
-  constexpr int C = 32 * kStandaloneV;
+  constexpr int C = 32 * kClusterV;
   const int nc = (base.m + C - 1) / C;
   const int c0 = static_cast<int>(static_cast<long long>(nc) * rank / size);
   const int c1 = static_cast<int>(static_cast<long long>(nc) * (rank + 1) / size);
@@ -1158,7 +1178,7 @@ __global__ void __launch_bounds__(NT + 32, 1)
   if (threadIdx.x >= NT) {
     if (threadIdx.x == NT) producer_entry<Real>(slice, L, smem, chain_local);
   } else {
-    run_consumers<Real, NT, R, kStandaloneV, false, true, true, true>(slice, L, smem, chain_local, &cx);
+    run_consumers<Real, NT, R, kClusterV, false, true, true, true>(slice, L, smem, chain_local, &cx);
   }
   cluster_sync_all();
 }
@@ -1186,13 +1206,14 @@ int launch_one_cluster(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg
   return e == cudaSuccess ? NAJA_OK : NAJA_ERR_CUDA;
 }
 
-template <class Real, int NT, int R>
+template <class Real, int NT, int R, bool UNI = false>
 int launch_one(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream) {
   if constexpr (NT == 128 || NT == 256) {
-    if (cfg.cluster > 1) return launch_one_cluster<Real, NT, R>(a, nchains, cfg, stream);
+    if (!UNI && cfg.cluster > 1) return launch_one_cluster<Real, NT, R>(a, nchains, cfg, stream);
   }
   if (cfg.cluster > 1) return NAJA_ERR_UNSUPPORTED;
-  auto kern = chr_kernel<Real, NT, R>;
+  if (UNI && a.m % kStandaloneV<Real> != 0) return NAJA_ERR_UNSUPPORTED;
+  auto kern = chr_kernel<Real, NT, R, UNI>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(cfg.smem));
   if (e != cudaSuccess) return NAJA_ERR_CUDA;
   const Layout L = make_layout(a.d, a.lda, sizeof(Real), NT, cfg.slots);
@@ -1203,6 +1224,21 @@ int launch_one(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaSt
 // cfg.rows = chunks per warp (template capacity).
 template <class Real, int NT>
 int launch_rows(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream) {
+  if (cfg.uniform) {
+    // cfg.rows = chunks of every warp (exact)
+    switch (cfg.rows) {
+      case 1: return launch_one<Real, NT, 1, true>(a, nchains, cfg, stream);
+      case 2: return launch_one<Real, NT, 2, true>(a, nchains, cfg, stream);
+      case 3: return launch_one<Real, NT, 3, true>(a, nchains, cfg, stream);
+      case 4: return launch_one<Real, NT, 4, true>(a, nchains, cfg, stream);
+      case 5: return launch_one<Real, NT, 5, true>(a, nchains, cfg, stream);
+      case 6: return launch_one<Real, NT, 6, true>(a, nchains, cfg, stream);
+      case 7: return launch_one<Real, NT, 7, true>(a, nchains, cfg, stream);
+      case 8: return launch_one<Real, NT, 8, true>(a, nchains, cfg, stream);
+      default: return NAJA_ERR_UNSUPPORTED;
+    }
+  }
+  // cfg.rows = chunks per warp (template capacity)
   switch (cfg.rows) {
     case 1: return launch_one<Real, NT, 1>(a, nchains, cfg, stream);
     case 2: return launch_one<Real, NT, 2>(a, nchains, cfg, stream);

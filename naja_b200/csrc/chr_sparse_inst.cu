@@ -49,6 +49,7 @@ int chr_sparse_plan(int precision, int m, int d, int max_col, double mean_col, i
   out->slice_lda = 0;
   out->max_col = max_col;
   out->pair_scatter = scatter ? 1 : 0;
+  out->uniform = 0;
   return NAJA_OK;
 }
 

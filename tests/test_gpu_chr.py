@@ -194,3 +194,34 @@ def test_cluster_rejects_bad_size(cuda):
     P = Polytope(A, b)
     with pytest.raises(InvalidArgument, match="cluster"):
         P.run(x0, 10, 1, 2, cluster=9)
+
+
+@pytest.mark.parametrize("extra_rows", [0, 1, 2, 3])
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_dense_kernel_row_counts(cuda, extra_rows, precision):
+    """The dense kernel at m % 4 = 0..3 and several thread counts: uniform
+    chunks (every warp the same straight-line row pass, the rows past m
+    repeating the last ones; m a multiple of the rows per lane) and the
+    row-count-tested chunks give the oracle's samples and final slack."""
+    import torch
+
+    g = synth.genome_shaped(n=600, d=90, density=0.1, seed_T=8, seed_u=9)
+    A = np.vstack([g["A"], g["A"][:extra_rows] * 0.5])
+    b = np.concatenate([g["b"], g["b"][:extra_rows] * 0.5 + 1.0])
+    P = Polytope(A, b)
+    kw = dict(seed=4, pair_prob=0.3, resync_interval=40, ksparse_prob=0.1, ksparse_k=3)
+    ref = O.chr_run(A, b, g["start"], 30, 6, 3, precision=precision, **kw)
+    sfs = []
+    for tpb in (64, 256, 512):
+        sf = torch.empty((3, P.m), dtype=torch.float64 if precision == "fp64" else torch.float32, device="cuda")
+        xf = np.empty((3, P.d))
+        got = P.run(g["start"], 30, 6, 3, precision=precision, out_dtype="f64", sparse="dense", tpb=tpb,
+                    X_final=xf, slack_final=sf, **kw)
+        P.check()
+        assert np.array_equal(got, ref), (tpb, np.abs(got - ref).max())
+        sfs.append(sf)
+    # every thread count leaves the same final slack, close to b - A x_final
+    assert all(torch.equal(sfs[0], s) for s in sfs[1:])
+    exact = b - xf @ A.T
+    tol = 1e-9 if precision == "fp64" else 1e-3
+    assert np.abs(sfs[0].cpu().numpy() - exact).max() <= tol * max(1.0, np.abs(b).max())
