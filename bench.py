@@ -57,12 +57,13 @@ METRIC = "min-ESS/sec at split-R-hat<1.01, learned-rounded vs plain CHR, 1 B200"
 UNIT = "min-ESS/s"
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) of one launch of the headline step kernel,
-# chr_kernel<float, 512, 8> on the rounded genome-shaped job (n 2600, d 700,
-# 16 chains x 12,500 samples, thinning 116, pair 0.3, resync 2048, FP32,
-# Philox seed 0): one ncu capture of the full-size launch with
-# dram__bytes_read.sum 84.34 MB + dram__bytes_write.sum 549.55 MB.  Reported
-# as roofline.traffic only for that exact workload.
-HEADLINE_TRAFFIC_BYTES = 84.34e6 + 549.55e6
+# chr_kernel<float, 512, 3, uniform> on the rounded genome-shaped job (n
+# 2600, d 700, 16 chains x 12,500 samples, thinning 116, pair 0.3, resync
+# 2048, FP32, Philox seed 0), which runs as 709 launches of 2,048 steps:
+# one 1-pass ncu capture of a whole job's launches gave
+# dram__bytes_read.sum 10.76 GB + dram__bytes_write.sum 1.5 KB over 709.
+# Reported as roofline.traffic only for that exact workload.
+HEADLINE_TRAFFIC_BYTES = 10.76e9 / 709 + 1.5e3 / 709
 
 
 def _peaks():
@@ -320,7 +321,9 @@ def _compact(line):
             "tier,K,t/fp64,drift_rel,agree_step,viol": [
                 [r["tier"], r["K"], _r(r.get("time_vs_fp64", 1.0), 3), _r(r["slack_drift"]["max_rel"], 2),
                  r.get("agree_1e-3_through_step_min", 0), r["bound_violations"]] for r in ps["chr"]],
-            "backmap_ms_maxrel": {m: [_r(v["ms_200k"], 3), _r(v["max_rel"], 2)] for m, v in ps["backmap"].items()}}
+            # C3 backmap ms / max rel. error per mode: tc modes only (the full table is in the detail file)
+            "bm_ms_maxrel": {m: [_r(v["ms_200k"], 3), _r(v["max_rel"], 2)] for m, v in ps["backmap"].items()
+                             if m in ("bf16x3", "tf32x3")}}
     if "learned_rounding" in line:
         lr = line["learned_rounding"]
         out["learned_rounding"] = {
@@ -400,7 +403,7 @@ def _ours(a, rank, world):
     W = Workload(a)
     # the rounding y = M z + c, the rounded polytope and the composed backmap
     # T' = T M, shift' = T c + shift are set up once (untimed here; e2e times them)
-    R = ng.make_rounding(a.rounding, W.A, W.b, W.start)
+    R = ng.make_rounding(a.rounding, W.A, W.b, W.start, device=dev.index)
     rounded = R.info["method"] != "identity"
     P = nb.Polytope(R.A, R.b, device=dev.index)
     Tp, shp = R.compose_backmap(W.T, W.shift)
@@ -469,6 +472,7 @@ def _ours(a, rank, world):
                              precision=a.precision, sparse=a.sparse, tpb=a.tpb)
     chr_mean = statistics.mean(chr_ms)
     achieved = W.bytes_per_step * W.steps / (chr_mean / 1e3) / 1e9
+    n_chr = _chr_launches(W, a, choice)
     steps_per_s = W.steps * world / (ms_per_step / 1e3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
@@ -483,7 +487,10 @@ def _ours(a, rank, world):
                      "bytes_definition": "4 m (1 + p_pair) + 4 d / thinning: one FP32 column per coordinate step, "
                                          "two per pair step, plus the amortised sample write",
                      "compressed_bytes_per_chr_step": W.compressed_bytes_per_step,
-                     "chr_steps_per_launch": W.steps},
+                     # the job's step-kernel launches (one per recompute interval when segmented);
+                     # achieved is their aggregate rate, traffic one launch's DRAM bytes
+                     "chr_steps_per_launch": a.resync * W.nchains if n_chr > 1 else W.steps,
+                     "launches_per_job": n_chr // 2 if n_chr > 1 else 1},
         "chr_steps_per_s": steps_per_s, "min_ess": min_ess,
         "rounding": {k: v for k, v in R.info.items() if k in ("method", "newton_iterations", "seconds")},
         "job_ms": _stats(job_ms), "chr_ms": _stats(chr_ms),
@@ -532,8 +539,9 @@ def _ours(a, rank, world):
 
 def _e2e(a, W, torch, dev, min_ess):
     """The same job from host buffers through the public API, wall-clock per
-    job: the rounding (host FP64: analytic centre, barrier Hessian, its
-    inverse square root, A M and T M), the rounded polytope's upload, then
+    job: the rounding (FP64 on the GPU for dikin_full: analytic centre,
+    barrier Hessian, its inverse square root, A M and T M), the polytope's
+    creation, then
     sampling, backmap and the copy of every back-mapped sample to pinned
     host memory overlapped chunk by chunk (naja_chr_run_backmapped)."""
     import naja_b200 as nb
@@ -545,10 +553,19 @@ def _e2e(a, W, torch, dev, min_ess):
     for k in range(a.warmup + a.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        R = ng.make_rounding(a.rounding, W.A, W.b, W.start)
-        Tp, shp = R.compose_backmap(W.T, W.shift)
+        R = ng.make_rounding(a.rounding, W.A, W.b, W.start, device=dev.index)
         z0 = np.ascontiguousarray(np.broadcast_to(R.z0, (W.nchains, W.d)))
-        P = nb.Polytope(R.A, R.b, device=dev.index)
+        dv = R.info.get("dev")
+        if dv is not None:
+            # rounded on the GPU: compose T' = T M, shift' = T c + shift there too
+            T_d = torch.from_numpy(W.T).to(dev)
+            Tp, shp = T_d @ dv["M"], T_d @ dv["c"] + torch.from_numpy(W.shift).to(dev)
+            P = nb.Polytope(dv["A"], dv["b"], device=dev.index)
+            h2d = W.A.nbytes + W.b.nbytes + W.T.nbytes + W.shift.nbytes + z0.nbytes
+        else:
+            Tp, shp = R.compose_backmap(W.T, W.shift)
+            P = nb.Polytope(R.A, R.b, device=dev.index)
+            h2d = R.A.nbytes + R.b.nbytes + z0.nbytes + Tp.nbytes + shp.nbytes
         # sampling, backmap and copy to host overlapped chunk by chunk (same samples as one launch)
         sample_backmapped(P, Tp, shp, z0, W.nspc, W.thin, W.nchains, pinned_out, mode=a.backmap_mode,
                           seed=a.seed, pair_prob=W.pair, resync_interval=a.resync, precision=a.precision,
@@ -556,14 +573,13 @@ def _e2e(a, W, torch, dev, min_ess):
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         P.close()
-        h2d = R.A.nbytes + R.b.nbytes + z0.nbytes + Tp.nbytes + shp.nbytes
         if k >= a.warmup:
             times.append(dt * 1e3)
     ms = statistics.mean(times)
     return {"value": min_ess / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(pinned_out.numel() * 4), "ms_per_step": ms,
-            "timing": "wall clock per job with a device synchronise on both sides; rounding computed on the host "
-                      "inside the timed region"}
+            "timing": "wall clock per job with a device synchronise on both sides; rounding (FP64 on the GPU for "
+                      "dikin_full) inside the timed region"}
 
 
 def _plain_figure(a, W, torch, dev):

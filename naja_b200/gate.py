@@ -32,9 +32,10 @@ from .validate import ess_rhat
 ESS_MAX_SERIES = 48 * 1024
 
 
-def make_rounding(method, A, b, start):
+def make_rounding(method, A, b, start, device=None):
     """Rounding for `method`: "none", "dikin" (the reference's preconditioner)
-    or "dikin_full" (whole Dikin ellipsoid); a Rounding passes through."""
+    or "dikin_full" (whole Dikin ellipsoid; on the GPU when `device` is
+    given); a Rounding passes through."""
     if isinstance(method, rnd.Rounding):
         return method
     if method in (None, "none", "plain"):
@@ -42,7 +43,7 @@ def make_rounding(method, A, b, start):
     if method == "dikin":
         return rnd.dikin(A, b, start)
     if method == "dikin_full":
-        return rnd.dikin_full(A, b, start)
+        return rnd.dikin_full(A, b, start, device=device)
     raise ValueError(f"unknown rounding {method!r}")
 
 

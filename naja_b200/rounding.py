@@ -182,13 +182,20 @@ def _sym_sqrt(S, inverse=False):
     return (V * (ev ** (-0.5 if inverse else 0.5))) @ V.T
 
 
-def dikin_full(A, b, x0=None) -> Rounding:
+def dikin_full(A, b, x0=None, device=None) -> Rounding:
     """Whole-ellipsoid Dikin rounding: y = H^{-1/2} z + x_c with x_c the
     analytic centre and H = A^T S^-2 A its barrier Hessian (S = diag(b - A
     x_c)).  The Dikin ellipsoid {(y - x_c)^T H (y - x_c) <= 1}, which lies
     inside the polytope, becomes the unit ball in z, along every direction at
     once -- where dikin() stretches at most k_directions eigen-directions by a
-    clipped factor (the reference's preconditioner)."""
+    clipped factor (the reference's preconditioner).
+
+    device: a CUDA device (index or torch.device) computes the same steps in
+    FP64 on the GPU (cuBLAS / cuSOLVER through torch): the same rounding up
+    to rounding differences in the last digits, in a fraction of the host's
+    time for genome-scale A."""
+    if device is not None:
+        return _dikin_full_gpu(A, b, x0, device)
     A = np.asarray(A, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     t0 = _now()
@@ -198,6 +205,51 @@ def dikin_full(A, b, x0=None) -> Rounding:
     M = _sym_sqrt(H, inverse=True)
     return Rounding(M, x_c, A @ M, s.copy(), np.zeros(A.shape[1]),
                     {"method": "dikin_full", "newton_iterations": iters, "seconds": _now() - t0})
+
+
+def _dikin_full_gpu(A, b, x0, device, tol: float = 1e-9, max_iter: int = 200) -> Rounding:
+    """dikin_full's steps (analytic_center's damped Newton, the Hessian, its
+    inverse square root by eigendecomposition, A M) in FP64 on `device`."""
+    import torch
+
+    dev = torch.device("cuda", device) if isinstance(device, int) else torch.device(device)
+    t0 = _now()
+    At = torch.as_tensor(np.asarray(A, dtype=np.float64), device=dev)
+    bt = torch.as_tensor(np.asarray(b, dtype=np.float64).reshape(-1), device=dev)
+    d = At.shape[1]
+    x = torch.zeros(d, dtype=torch.float64, device=dev) if x0 is None else \
+        torch.as_tensor(np.asarray(x0, dtype=np.float64).reshape(-1), device=dev).clone()
+    s = bt - At @ x
+    if not bool((s > 0).all()):
+        raise ValueError("analytic_center: the start point is not strictly feasible")
+    it = 0
+    for it in range(1, max_iter + 1):
+        w = 1.0 / s
+        g = At.T @ w
+        Aw = At * w[:, None]
+        L = torch.linalg.cholesky(Aw.T @ Aw)
+        dx = -torch.cholesky_solve(g[:, None], L)[:, 0]
+        lam2 = float(-(g @ dx))
+        if lam2 <= tol * tol:
+            break
+        Adx = At @ dx
+        t = 1.0 / (1.0 + lam2 ** 0.5)
+        pos = Adx > 0
+        if bool(pos.any()):
+            t = min(t, 0.99 * float((s[pos] / Adx[pos]).min()))
+        x = x + t * dx
+        s = bt - At @ x
+    Aw = At * (1.0 / s)[:, None]
+    ev, V = torch.linalg.eigh(Aw.T @ Aw)
+    ev = torch.clamp(ev, min=float(ev.max()) * 1e-14)
+    M = (V * ev.rsqrt()) @ V.T
+    AM = At @ M
+    # the device copies stay in info["dev"] for callers that keep working on the GPU
+    out = Rounding(M.cpu().numpy(), x.cpu().numpy(), AM.cpu().numpy(), s.cpu().numpy(), np.zeros(d),
+                   {"method": "dikin_full", "newton_iterations": it, "device": str(dev),
+                    "dev": {"M": M, "c": x, "A": AM, "b": s}})
+    out.info["seconds"] = _now() - t0
+    return out
 
 
 def from_covariance(A, b, cov, c, y0=None) -> Rounding:

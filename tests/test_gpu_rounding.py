@@ -55,3 +55,20 @@ def test_sample_to_gate_stops_at_budget(cuda):
                               resync_interval=200, budget_s=0.5, max_chunks=3)
     assert out["chunks"] <= 3 and len(out["curve"]) == out["chunks"]
     assert out["bounds_violations"] == 0
+
+
+def test_dikin_full_on_the_gpu_matches_the_host(cuda):
+    """dikin_full(device=0) takes the host's steps in FP64 on the GPU: the same
+    centre, M and rounded polytope up to rounding in the last digits."""
+    from naja_b200 import rounding, synth
+
+    g = synth.genome_shaped(n=900, d=240, density=0.08, seed_T=6, seed_u=7)
+    start = g["start"] + 1e-3  # off the centre, so Newton takes several steps
+    cpu = rounding.dikin_full(g["A"], g["b"], start)
+    gpu = rounding.dikin_full(g["A"], g["b"], start, device=0)
+    assert gpu.info["newton_iterations"] == cpu.info["newton_iterations"] > 1
+    for name in ("M", "c", "A", "b"):
+        x, y = getattr(cpu, name), getattr(gpu, name)
+        assert np.abs(x - y).max() <= 1e-9 * max(1.0, np.abs(x).max()), name
+    dv = gpu.info["dev"]
+    assert np.array_equal(dv["A"].cpu().numpy(), gpu.A)
