@@ -219,7 +219,7 @@ def _headline_traffic(a, W, choice):
     launch's workload (else None: traffic was not captured for it)."""
     same = (W.n, W.d, W.nchains, W.nspc, W.thin, W.pair, a.resync, a.precision, a.seed, a.rounding) == \
         (2600, 700, 16, 12500, 116, 0.3, 2048, "fp32", 0, "dikin_full")
-    return HEADLINE_TRAFFIC_BYTES if same and choice["kernel"] != "columns" and choice["threads"] == 512 else None
+    return HEADLINE_TRAFFIC_BYTES if same and choice["kernel"] != "columns" and choice["threads"] == 448 else None
 
 
 def _dgemm_backmap_ms(torch, T_dev, sh_dev, Z):

@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # (__fma_rn / __fmaf_rn); nothing else may be contracted, so the device
 # arithmetic is reproducible bit for bit by the CPU restatement.
 BASE = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include")]
-CHR_THREADS = (32, 64, 128, 256, 512, 992)
+CHR_THREADS = (32, 64, 128, 256, 448, 512, 992)
 
 
 def _units():

@@ -9,12 +9,14 @@ int chr_launch_float_32(const ChrArgs& a, int nchains, const ChrLaunchConfig& cf
 int chr_launch_float_64(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
 int chr_launch_float_128(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
 int chr_launch_float_256(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+int chr_launch_float_448(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
 int chr_launch_float_512(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
 int chr_launch_float_992(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
 int chr_launch_double_32(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
 int chr_launch_double_64(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
 int chr_launch_double_128(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
 int chr_launch_double_256(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
+int chr_launch_double_448(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
 int chr_launch_double_512(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
 int chr_launch_double_992(const ChrArgs& a, int nchains, const ChrLaunchConfig& cfg, cudaStream_t stream);
 
@@ -172,6 +174,16 @@ int plan_single(int precision, int m, int d, int lda, int tpb, int max_slots, Ch
   if (m % v == 0 && m >= v && exact <= kMaxUniformChunks && exact <= max_chunks_for(threads, v)) {
     out->uniform = 1;
     out->rows = exact;
+    // 14 warps where they hold the same chunks per warp as 16: fewer row
+    // slots repeat (m 5200: 42 for 41 chunks instead of 48); the layout
+    // depends on the thread count, so it is planned again
+    if (tpb <= 0 && threads == 512 && 14 * exact >= chunks) {
+      const Layout L448 = make_layout(d, lda, elt, 448, slots);
+      if (L448.total <= kSmemBudget) {
+        out->threads = 448;
+        out->smem = L448.total;
+      }
+    }
   }
   return NAJA_OK;
 }
@@ -240,6 +252,7 @@ int chr_launch(int precision, const ChrArgs& args, int nchains, const ChrLaunchC
     case 64: return f64 ? chr_launch_double_64(args, nchains, cfg, stream) : chr_launch_float_64(args, nchains, cfg, stream);
     case 128: return f64 ? chr_launch_double_128(args, nchains, cfg, stream) : chr_launch_float_128(args, nchains, cfg, stream);
     case 256: return f64 ? chr_launch_double_256(args, nchains, cfg, stream) : chr_launch_float_256(args, nchains, cfg, stream);
+    case 448: return f64 ? chr_launch_double_448(args, nchains, cfg, stream) : chr_launch_float_448(args, nchains, cfg, stream);
     case 512: return f64 ? chr_launch_double_512(args, nchains, cfg, stream) : chr_launch_float_512(args, nchains, cfg, stream);
     case 992: return f64 ? chr_launch_double_992(args, nchains, cfg, stream) : chr_launch_float_992(args, nchains, cfg, stream);
     default: return NAJA_ERR_UNSUPPORTED;

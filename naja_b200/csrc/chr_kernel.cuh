@@ -621,6 +621,8 @@ struct ClusterCtx {
 // repeat the last V rows (m % V == 0 keeps that group aligned and whole),
 // whose ratios, slack and updates are bit for bit those of the rows they
 // repeat, so the extremes are unchanged; only the owner of a row writes it.
+// (Skipping a last chunk that would only repeat rows, by a warp-uniform
+// test, was measured 1.4 % slower at the headline shape.)
 template <class Real, int NT, int R, int V, bool SS = false, bool TIMING = true, bool MAYBE_DIRECT = true,
           bool CL = false, bool FUSED = false, bool UNI = false>
 __device__ void run_consumers(const ChrArgs& a, const Layout& L, unsigned char* smem, int chain_local,

@@ -41,7 +41,7 @@ def test_rounded_headline_shape_fp32_matches_oracle(cuda, rounded):
     kw = dict(seed=0, pair_prob=0.3, resync_interval=2048, precision="fp32")
     nspc, thin, nch = 20, 116, 16  # 2,320 steps: segments of 2,048 and 272 steps
     choice = P.kernel_choice(12500, thin, nch, **kw)
-    assert choice["kernel"] == "dense" and choice["threads"] == 512, choice
+    assert choice["kernel"] == "dense" and choice["threads"] == 448, choice
     xf = np.empty((nch, R.A.shape[1]))
     got = P.run(R.z0, nspc, thin, nch, out_dtype="f64", X_final=xf, **kw)
     P.check()
