@@ -57,13 +57,13 @@ METRIC = "min-ESS/sec at split-R-hat<1.01, learned-rounded vs plain CHR, 1 B200"
 UNIT = "min-ESS/s"
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes (read + write) of one launch of the headline step kernel,
-# chr_kernel<float, 512, 3, uniform> on the rounded genome-shaped job (n
+# chr_kernel<float, 448, 3, uniform> on the rounded genome-shaped job (n
 # 2600, d 700, 16 chains x 12,500 samples, thinning 116, pair 0.3, resync
 # 2048, FP32, Philox seed 0), which runs as 709 launches of 2,048 steps:
 # one 1-pass ncu capture of a whole job's launches gave
-# dram__bytes_read.sum 10.76 GB + dram__bytes_write.sum 1.5 KB over 709.
+# dram__bytes_read.sum 10.766 GB + dram__bytes_write.sum 22.5 KB over 709.
 # Reported as roofline.traffic only for that exact workload.
-HEADLINE_TRAFFIC_BYTES = 10.76e9 / 709 + 1.5e3 / 709
+HEADLINE_TRAFFIC_BYTES = 10.766e9 / 709 + 22.5e3 / 709
 
 
 def _peaks():
