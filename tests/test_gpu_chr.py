@@ -220,6 +220,9 @@ def test_dense_kernel_row_counts(cuda, extra_rows, precision):
         P.check()
         assert np.array_equal(got, ref), (tpb, np.abs(got - ref).max())
         sfs.append(sf)
+    # columns read straight from global memory (a ring of fewer than 3 slots)
+    direct = P.run(g["start"], 30, 6, 3, precision=precision, out_dtype="f64", sparse="dense", max_slots=2, **kw)
+    assert np.array_equal(direct, ref)
     # every thread count leaves the same final slack, close to b - A x_final
     assert all(torch.equal(sfs[0], s) for s in sfs[1:])
     exact = b - xf @ A.T
