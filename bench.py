@@ -205,11 +205,11 @@ def _backmap_error(torch, Tm, shift, samples_dev, V_dev, mode):
 
 
 def _chr_launches(W, a, choice):
-    """Kernels one CHR run launches: a dense run with a recompute interval K
+    """Kernels one CHR run launches: a run with a recompute interval K
     shorter than the run and m d >= 2^19 runs in segments of K steps, each a
-    slack-recompute kernel and a step kernel."""
+    slack-recompute kernel and a step kernel (either step kernel)."""
     total = W.nspc * W.thin
-    if choice["kernel"] == "dense" and 0 < a.resync < total and W.m * W.d >= (1 << 19):
+    if 0 < a.resync < total and W.m * W.d >= (1 << 19):
         return 2 * (-(-total // a.resync))
     return 1
 

@@ -645,10 +645,12 @@ int naja_chr_run(const naja_polytope* P, const naja_chr_params* p, const double*
   a.slack_final = dsf;
 
   const long long total_steps = static_cast<long long>(p->nspc) * p->thinning;
-  if (use_sparse)
+  const bool segments =
+      chr_use_segments(P->m, d, p->resync_interval, total_steps, cfg.cluster, p->wait_cycles != nullptr);
+  if (segments)
+    st = chr_run_segmented(p->precision, a, p->nchains, cfg, stream, nullptr, use_sparse ? &spa : nullptr);
+  else if (use_sparse)
     st = chr_sparse_launch(p->precision, a, spa, p->nchains, cfg, stream);
-  else if (chr_use_segments(P->m, d, p->resync_interval, total_steps, cfg.cluster, p->wait_cycles != nullptr))
-    st = chr_run_segmented(p->precision, a, p->nchains, cfg, stream, nullptr);
   else
     st = chr_launch(p->precision, a, p->nchains, cfg, stream);
   if (st) {

@@ -121,19 +121,23 @@ int chr_launch(int precision, const ChrArgs& args, int nchains, const ChrLaunchC
 // own.  Samples, final positions, final slack and RNG streams are those of
 // the single launch, bit for bit; the recompute, which the step kernel
 // does on the chain's one SM, reads A64 on every SM instead.  Returns the
-// number of kernel launches through `launches` (nullable).
+// number of kernel launches through `launches` (nullable).  `sp` non-null:
+// the segments run the compressed-column kernel (chr_sparse_launch) with
+// those columns; its own recompute skips the zero terms of a row, which can
+// change only the sign of a zero sum, so against the dense recompute here it
+// can differ at most in the sign of a zero slack (where b is -0).
 int chr_run_segmented(int precision, const ChrArgs& args, int nchains, const ChrLaunchConfig& cfg,
-                      cudaStream_t stream, long long* launches);
+                      cudaStream_t stream, long long* launches, const SpArgs* sp = nullptr);
 
 // Steps of one launch (host side of the kernels' launch_steps).
 inline long long launch_steps_host(const ChrArgs& a) {
   return a.steps > 0 ? a.steps : static_cast<long long>(a.nspc) * a.thinning;
 }
 
-// True where chr_run_segmented pays for its per-segment launches: a dense
-// single-CTA run with a recompute interval shorter than the run and an A64
-// large enough (m d >= kSegmentMinCells) that reading it from one SM costs
-// more than a segment boundary.
+// True where chr_run_segmented pays for its per-segment launches: a
+// single-CTA run (either step kernel) with a recompute interval shorter than
+// the run and an A64 large enough (m d >= kSegmentMinCells) that
+// recomputing from one SM costs more than a segment boundary.
 constexpr long long kSegmentMinCells = 1LL << 19;
 inline bool chr_use_segments(long long m, long long d, int resync, long long total_steps, int cluster,
                              bool instrumented) {

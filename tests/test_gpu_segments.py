@@ -67,16 +67,18 @@ def test_rounded_headline_shape_fp64_mrg_matches_reference_kernel(cuda, rounded)
     assert np.array_equal(_single_launch(P, R.z0, nspc, thin, nchains=nch, **kw), got)
 
 
+@pytest.mark.parametrize("sparse", ["dense", "columns"])
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
-def test_ragged_segments_and_final_slack(cuda, precision):
+def test_ragged_segments_and_final_slack(cuda, precision, sparse):
     """K = 100 with thinning 7 over 350 steps: segments of 100, 100, 100 and
-    50 steps, samples saved inside segments; the final slack too."""
+    50 steps, samples saved inside segments; the final slack too; for the
+    dense and the compressed-column step kernel."""
     import torch
 
     g = synth.genome_shaped(n=1300, d=420, density=0.1, seed_T=4, seed_u=5)  # m d = 1,092,000
     P = Polytope(g["A"], g["b"])
     nch, nspc, thin, K = 4, 50, 7, 100
-    kw = dict(seed=11, pair_prob=0.3, resync_interval=K, precision=precision, sparse="dense", out_dtype="f64")
+    kw = dict(seed=11, pair_prob=0.3, resync_interval=K, precision=precision, sparse=sparse, out_dtype="f64")
     dt = torch.float64 if precision == "fp64" else torch.float32
     sf = torch.empty((nch, P.m), dtype=dt, device="cuda")
     got = P.run(g["start"], nspc, thin, nch, slack_final=sf, **kw)
