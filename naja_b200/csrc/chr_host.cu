@@ -311,7 +311,8 @@ int chr_run_segmented(int precision, const ChrArgs& a0, int nchains, const ChrLa
     a.resync = 0;  // this segment's recompute is the one just made
     a.slack_final = s + 1 == nseg ? a0.slack_final : nullptr;
     if (own_states) a.rng_state = rs;
-    st = sp ? chr_sparse_launch(precision, a, *sp, nchains, cfg, stream) : chr_launch(precision, a, nchains, cfg, stream);
+    st = sp ? chr_sparse_launch(precision, a, *sp, nchains, cfg, stream)
+            : chr_launch(precision, a, nchains, cfg, stream);
     n_launch += 2;
   }
   if (!st && a0.X_final) {
