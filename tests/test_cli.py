@@ -142,3 +142,54 @@ def test_bulk_usage_and_contract_errors(tmp_path):
     r = _run("sample", "bulk", "--models-root", root, "--model-list", empty, "--out-root", tmp_path / "out",
              "--name", "RUN", "--gpus", "0", "--n-chains", 1, "--n-samples", 1, "--dry-run")
     assert r.returncode == 1
+
+
+def test_bulk_skip_existing_and_failures_on_the_host(tmp_path):
+    """--skip-existing takes a model as done when one of its job directories
+    holds non-empty samples.npy and profile.json (plus valid_mask.npy,
+    valid_fraction.txt and bounds_report.json under the bounds filter); the
+    newest such directory is reported.  A model that is not done runs, and
+    here (no GPU) fails on its own: FAIL with its message in
+    bulk_summary.csv, the others SKIP, exit status 1."""
+    import os
+    import time
+
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("the failing job needs a host without a GPU")
+    names = ("M1", "M2", "M3")
+    for n in names:
+        _model(tmp_path, n, backmap=True)
+    root, lst = tmp_path / "models", tmp_path / "models.txt"
+    lst.write_text("\n".join(names) + "\n")
+    for n in names:
+        (root / n / "rounding" / "INHERITED_FROM.txt").write_text("base_model_dir=/models/base\n")
+    run = tmp_path / "out" / "RUN_20260101_001"
+    files = ("samples.npy", "profile.json")
+    filt = ("valid_mask.npy", "valid_fraction.txt", "bounds_report.json")
+    for n in names:
+        for idx, extra in ((1, ()), (2, filt)):
+            job = run / n / f"{n}_20260101_00{idx}"
+            job.mkdir(parents=True)
+            for f in files + extra:
+                (job / f).write_text("x")
+            os.utime(job, (time.time() - 100 * (3 - idx), time.time() - 100 * (3 - idx)))
+    (run / "M3" / "M3_20260101_002" / "samples.npy").write_text("")  # empty: not complete
+    (run / "M3" / "M3_20260101_001" / "profile.json").unlink()
+    r = _run("sample", "bulk", "--models-root", root, "--model-list", lst, "--resume-from", run, "--name", "RUN",
+             "--gpus", "0", "--n-chains", 1, "--n-samples", 2, "--skip-existing")
+    assert r.returncode == 1 and "bulk sampling failed" in r.stderr
+    assert r.stdout.count("-> SKIP") == 2 and "M3 -> FAIL" in r.stdout
+    rows = {line.split(",")[0]: line.split(",") for line in (run / "bulk_summary.csv").read_text().splitlines()[1:]}
+    assert rows["M1"][1] == rows["M2"][1] == "SKIP" and rows["M3"][1] == "FAIL"
+    assert rows["M1"][5].endswith("M1_20260101_002")  # the newest complete directory
+    assert rows["M3"][4] and rows["M3"][5].startswith(str(run / "M3" / "M3_"))
+    assert all(r_[6] == "/models/base" for r_ in rows.values())
+    # under the bounds filter only directories with the filter's outputs count
+    (run / "M1" / "M1_20260101_002" / "bounds_report.json").unlink()
+    r = _run("sample", "bulk", "--models-root", root, "--model-list", lst, "--resume-from", run, "--name", "RUN",
+             "--gpus", "0", "--n-chains", 1, "--n-samples", 2, "--skip-existing", "--backmap",
+             "--bounds-policy", "filter")
+    assert r.returncode == 1, r.stderr
+    assert "M2 -> SKIP" in r.stdout and "M1 -> FAIL" in r.stdout and "M3 -> FAIL" in r.stdout
