@@ -1,5 +1,5 @@
-"""The bench's printed line (CPU): from a full line recorded by a
-driver-shaped run (tests/data/bench_line_full.json, every section), the
+"""The bench's printed line (CPU): from a full line recorded by a run with
+every section (`--steps 20 --warmup 5`; tests/data/bench_line_full.json), the
 compacted line keeps every key of the bench contract and stays well under
 the 3,000 characters of a log tail."""
 import importlib.util
